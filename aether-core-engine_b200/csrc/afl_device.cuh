@@ -1,0 +1,248 @@
+// afl_device.cuh -- device-side building blocks shared by every kernel.
+//
+// Layout: one scalar per cell, x fastest, idx = (k*ny + j)*nx + i, the
+// reference's layout (src/fluid.rs:88-90); u/v/w share the cell index
+// (src/fluid.rs:160-162, 341-343, 517-523).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace afl {
+
+struct Dims {
+  int nx, ny, nz;
+  int n;       // nx*ny*nz
+  int nxy;     // nx*ny
+  double h;
+};
+
+constexpr int kBlock = 256;          // threads per CTA of the flat kernels
+constexpr int kWarps = kBlock / 32;
+
+__host__ __device__ inline bool interior(const Dims &g, int i, int j, int k) {
+  return i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2 && k >= 1 && k <= g.nz - 2;
+}
+
+__device__ inline void decode(const Dims &g, int c, int &i, int &j, int &k) {
+  k = c / g.nxy;
+  const int r = c - k * g.nxy;
+  j = r / g.nx;
+  i = r - j * g.nx;
+}
+
+// f64::clamp / f32::clamp: "if x < lo {lo}; if x > hi {hi}".
+template <typename T>
+__device__ __forceinline__ T rs_clamp(T x, T lo, T hi) {
+  x = x < lo ? lo : x;
+  x = x > hi ? hi : x;
+  return x;
+}
+
+// Wall masks of enforce_wall_velocity_bc (src/fluid.rs:241-249): true where
+// the component is forced to zero.
+__device__ __forceinline__ bool wall_u(const Dims &g, int i, int j, int k) {
+  return i <= 1 || i + 1 >= g.nx || j == 0 || j + 1 >= g.ny || k == 0 || k + 1 >= g.nz;
+}
+__device__ __forceinline__ bool wall_v(const Dims &g, int i, int j, int k) {
+  return j <= 1 || j + 1 >= g.ny || i == 0 || i + 1 >= g.nx || k == 0 || k + 1 >= g.nz;
+}
+__device__ __forceinline__ bool wall_w(const Dims &g, int i, int j, int k) {
+  return k <= 1 || k + 1 >= g.nz || i == 0 || i + 1 >= g.nx || j == 0 || j + 1 >= g.ny;
+}
+
+// Corner cell and weights of the clamped trilinear footprint
+// (src/fluid.rs:95-108).
+template <typename T>
+struct Footprint {
+  int base;  // idx(i0, j0, k0)
+  T tx, ty, tz;
+};
+
+template <typename T>
+__device__ __forceinline__ Footprint<T> footprint(const Dims &g, T x, T y, T z) {
+  const T xc = rs_clamp(x, T(0.5), T(g.nx) - T(1.500001));
+  const T yc = rs_clamp(y, T(0.5), T(g.ny) - T(1.500001));
+  const T zc = rs_clamp(z, T(0.5), T(g.nz) - T(1.500001));
+  const int i0 = static_cast<int>(floor(xc));
+  const int j0 = static_cast<int>(floor(yc));
+  const int k0 = static_cast<int>(floor(zc));
+  Footprint<T> f;
+  f.base = (k0 * g.ny + j0) * g.nx + i0;
+  f.tx = xc - T(i0);
+  f.ty = yc - T(j0);
+  f.tz = zc - T(k0);
+  return f;
+}
+
+// sample_trilinear (src/fluid.rs:110-127): x-lerps, then y, then z, each as
+// a*(1-t) + b*t.
+template <typename T>
+__device__ __forceinline__ T trilinear(const T *__restrict__ f, const Dims &g,
+                                       const Footprint<T> &p) {
+  const int b = p.base, sx = 1, sy = g.nx, sz = g.nxy;
+  const T c000 = __ldg(f + b), c100 = __ldg(f + b + sx);
+  const T c010 = __ldg(f + b + sy), c110 = __ldg(f + b + sy + sx);
+  const T c001 = __ldg(f + b + sz), c101 = __ldg(f + b + sz + sx);
+  const T c011 = __ldg(f + b + sz + sy), c111 = __ldg(f + b + sz + sy + sx);
+  const T ox = T(1) - p.tx, oy = T(1) - p.ty, oz = T(1) - p.tz;
+  const T c00 = c000 * ox + c100 * p.tx;
+  const T c10 = c010 * ox + c110 * p.tx;
+  const T c01 = c001 * ox + c101 * p.tx;
+  const T c11 = c011 * ox + c111 * p.tx;
+  const T c0 = c00 * oy + c10 * p.ty;
+  const T c1 = c01 * oy + c11 * p.ty;
+  return c0 * oz + c1 * p.tz;
+}
+
+// stencil_minmax (src/fluid.rs:131-150): same 8 corners, fmin/fmax keep the
+// non-NaN operand like f64::min/max.
+template <typename T>
+__device__ __forceinline__ void minmax8(const T *__restrict__ f, const Dims &g,
+                                        int base, T &lo, T &hi) {
+  const int sy = g.nx, sz = g.nxy;
+  lo = T(INFINITY);
+  hi = T(-INFINITY);
+#pragma unroll
+  for (int dk = 0; dk <= 1; ++dk)
+#pragma unroll
+    for (int dj = 0; dj <= 1; ++dj)
+#pragma unroll
+      for (int di = 0; di <= 1; ++di) {
+        const T v = __ldg(f + base + dk * sz + dj * sy + di);
+        lo = fmin(lo, v);
+        hi = fmax(hi, v);
+      }
+}
+
+// ---- deterministic reductions ---------------------------------------------
+// Butterfly inside the warp, then the warp sums in warp order: the result is a
+// pure function of the per-thread inputs, so every CTA that reduces the same
+// data gets the same bits.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Sums NV values across the CTA; the result is valid in every thread.
+// `scratch` needs kWarps*NV doubles.  Ends with a __syncthreads.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < NV; ++a) v[a] = warp_sum(v[a]);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int a = 0; a < NV; ++a) scratch[warp * NV + a] = v[a];
+  __syncthreads();
+#pragma unroll
+  for (int a = 0; a < NV; ++a) {
+    double s = 0.0;
+    for (int w = 0; w < kWarps; ++w) s += scratch[w * NV + a];
+    v[a] = s;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ double block_max(double v, double *scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  double m = scratch[0];
+  for (int w = 1; w < kWarps; ++w) m = fmax(m, scratch[w]);
+  __syncthreads();
+  return m;
+}
+
+// Sums NV interleaved partials (parts[b*NV + a], b < nparts) in a fixed order;
+// every CTA calling this on the same data gets identical results.
+template <int NV>
+__device__ __forceinline__ void reduce_partials(const double *parts, int nparts,
+                                                double (&out)[NV], double *scratch) {
+#pragma unroll
+  for (int a = 0; a < NV; ++a) out[a] = 0.0;
+  for (int b = threadIdx.x; b < nparts; b += blockDim.x)
+#pragma unroll
+    for (int a = 0; a < NV; ++a) out[a] += __ldcg(parts + b * NV + a);
+  block_sum<NV>(out, scratch);
+}
+
+// ---- bounded grid barrier for the persistent (cooperative) kernels ---------
+// Sense-reversing barrier over `nblocks` co-resident CTAs.  The wait is
+// bounded by `timeout_ns` of %globaltimer; a CTA that gives up, or that sees
+// another CTA's abort, returns false and the kernel unwinds.  No wait in this
+// library is unbounded.
+struct GridSync {
+  unsigned int *count;   // arrivals in the current generation
+  unsigned int *gen;     // generation number
+  int *abort_flag;       // set to a non-zero code by the first CTA to give up
+  unsigned int nblocks;
+  unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ int ld_relaxed_i32(const int *p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release(unsigned int *p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Returns true when every CTA arrived; false on timeout/abort (code 1 =
+// timeout is recorded in abort_flag).
+__device__ inline bool grid_sync(const GridSync &gs) {
+  __shared__ int ok_shared;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned int g0 = ld_acquire(gs.gen);
+    __threadfence();
+    const unsigned int arrived = atomicAdd(gs.count, 1u);
+    if (arrived == gs.nblocks - 1) {
+      *gs.count = 0;
+      __threadfence();
+      st_release(gs.gen, g0 + 1u);
+    } else {
+      const unsigned long long t0 = global_ns();
+      unsigned int spins = 0;
+      while (ld_acquire(gs.gen) == g0) {
+        if (ld_relaxed_i32(gs.abort_flag) != 0) { ok = 0; break; }
+        if ((++spins & 63u) == 0 && global_ns() - t0 > gs.timeout_ns) {
+          atomicCAS(gs.abort_flag, 0, 1);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+    if (ld_relaxed_i32(gs.abort_flag) != 0) ok = 0;
+    ok_shared = ok;
+  }
+  __syncthreads();
+  return ok_shared != 0;
+}
+
+}  // namespace afl

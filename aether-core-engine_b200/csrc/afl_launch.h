@@ -1,0 +1,141 @@
+// afl_launch.h -- host-side launchers for the stage kernels.
+//
+// T is the storage/arithmetic type of velocity, density and temperature:
+// double for the FP64 drop-in form, float for the mixed form.  Pressure and
+// the Poisson right-hand side are always double.  Every launcher is
+// asynchronous on `st`.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "afl_device.cuh"
+
+namespace afl {
+
+// Device-resident per-step report written by the Poisson kernels (mirrors
+// afl_solve_info field for field).
+struct SolveReport {
+  int32_t iterations;
+  int32_t refinements;
+  int32_t converged;
+  int32_t status;
+  double initial_residual;
+  double final_residual;
+  double rhs_norm;
+};
+
+// Barrier + scratch state of the persistent kernels.
+struct PersistentState {
+  unsigned int *count;
+  unsigned int *gen;
+  int *abort_flag;
+  double *partials;      // >= 6 * max_blocks doubles (2 buffers x 3 values)
+  int max_blocks;
+  unsigned long long timeout_ns;
+};
+
+// Number of CTAs the reduction kernels use (fixed, so sums are reproducible).
+constexpr int kReduceBlocks = 592;  // 4 per SM on a 148-SM B200
+constexpr int kReduceMaxVals = 8;
+
+template <typename T>
+void launch_advect_fwd(const Dims &g, const T *u, const T *v, const T *w, const T *src,
+                       T *fwd, double dt, cudaStream_t st);
+template <typename T>
+void launch_advect_mc(const Dims &g, const T *u, const T *v, const T *w, const T *src,
+                      const T *fwd, T *out, double dt, double dissipation, bool nonneg,
+                      cudaStream_t st);
+template <typename T>
+void launch_wall_bc(const Dims &g, T *u, T *v, T *w, cudaStream_t st);
+template <typename T>
+void launch_curl(const Dims &g, const T *u, const T *v, const T *w, T *cx, T *cy, T *cz,
+                 T *cmag, cudaStream_t st);
+template <typename T>
+void launch_confine_buoy(const Dims &g, T *u, T *v, T *w, const T *rho, const T *temp,
+                         const T *cx, const T *cy, const T *cz, const T *cmag, double dt,
+                         double eps, double beta, double alpha, cudaStream_t st);
+// b = -h*(du+dv+dw) on the interior (0 elsewhere); partials get
+// (sum div^2, sum b^2) per CTA; finalize writes {rms, ||b||} to out2.
+template <typename T>
+void launch_divergence(const Dims &g, const T *u, const T *v, const T *w, double *b,
+                       double *partials, double *out2, cudaStream_t st);
+template <typename T>
+void launch_project(const Dims &g, T *u, T *v, T *w, const double *p, cudaStream_t st);
+template <typename T>
+void launch_inject_jet(const Dims &g, const int lo[3], const int hi[3], T *rho, T *temp,
+                       T *u, T *v, T *w, const double jet[6], double r2, double dt,
+                       double pulse, cudaStream_t st);
+template <typename T>
+void launch_inject_sphere(const Dims &g, const int lo[3], const int hi[3], T *rho,
+                          T *temp, const double *amp, const double c[3], double r2,
+                          double rho_val, double temp_val, cudaStream_t st);
+// Writes 8 doubles (time, KE, enstrophy, peak, mass, com xyz) to out8.
+template <typename T>
+void launch_telemetry(const Dims &g, const T *u, const T *v, const T *w, const T *rho,
+                      double time_sec, double *partials, double *out8, cudaStream_t st);
+template <typename T>
+void launch_max(const Dims &g, const T *x, double *partials, double *out1, cudaStream_t st);
+template <typename T>
+void launch_sample(const Dims &g, const T *f, const double *xyz, int npts, double *out,
+                   cudaStream_t st);
+// Precision conversions for the mixed form's uploads/downloads.
+void launch_convert_f64_to_f32(const double *src, float *dst, int n, cudaStream_t st);
+void launch_convert_f32_to_f64(const float *src, double *dst, int n, cudaStream_t st);
+
+// ---- Poisson ---------------------------------------------------------------
+struct CgArgs {
+  Dims g;
+  double *p;        // pressure (warm start in, solution out)
+  const double *b;  // right-hand side
+  double *r, *d0, *d1, *q;
+  int max_iters;
+  double rel_tol;
+  SolveReport *report;
+};
+// Returns the number of CTAs used (for tests/diagnostics).
+int launch_cg_f64(const CgArgs &a, const PersistentState &ps, cudaStream_t st);
+
+struct SorArgs {
+  Dims g;
+  double *p;
+  const double *b;
+  int sweeps;
+  double omega;
+  SolveReport *report;
+};
+int launch_rbsor_f64(const SorArgs &a, const PersistentState &ps, cudaStream_t st);
+
+struct MixedCgArgs {
+  Dims g;
+  double *p;          // f64 pressure
+  const double *b;    // f64 right-hand side
+  float *r, *e, *d0, *d1, *q;  // f32 inner-CG vectors
+  int max_inner;      // inner iterations per pass
+  int max_total;      // cap on inner iterations over all passes
+  int max_refine;
+  double inner_rel_tol;
+  double rel_tol;     // outer (f64) target
+  SolveReport *report;
+};
+int launch_cg_mixed(const MixedCgArgs &a, const PersistentState &ps, cudaStream_t st);
+
+struct SorMixedArgs {
+  Dims g;
+  double *p;
+  const double *b;
+  float *p32;
+  float *b32;
+  int sweeps;
+  double omega;
+  SolveReport *report;
+};
+int launch_rbsor_mixed(const SorMixedArgs &a, const PersistentState &ps, cudaStream_t st);
+
+// Occupancy-derived CTA count of each persistent kernel (co-residency bound).
+int persistent_blocks_cg_f64();
+int persistent_blocks_sor_f64();
+int persistent_blocks_cg_mixed();
+int persistent_blocks_sor_mixed();
+
+}  // namespace afl

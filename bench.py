@@ -1,0 +1,464 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 smoke step: Mcell-steps/s on the 128^3 plume.
+
+Workload (the configuration the headline metric is quoted on): a 128^3 MAC
+grid, seed-0 velocity noise in [-0.01, 0.01], a sphere source at
+(64, 12.8, 64) with radius 10 cells assigning density = temperature = 1 each
+step, alpha 0.08, beta 0.4, eps 0.3, dt = 0.5 h, 200 steps.  A "step" is one
+FluidSolver3D::step (advection of u, v, w; source; confinement + buoyancy;
+projection with the pressure solve; advection of density and temperature;
+telemetry).
+
+Forms measured in one run:
+  mixed_cg  (headline `value`)  f32 stencils/SpMV, f64 dots, f64 refinement to 1e-6
+  fp64_cg                      the plain f64 drop-in, CG to 1e-6 (max 200)
+  fp64_sor / mixed_sor         red-black SOR omega = 1.7, 80 sweeps per step
+Each form runs W untimed warm-up steps, is re-initialised (outside the timed
+region) and then times exactly K steps from the initial state on the device
+(CUDA events on the solver's stream, barrier + synchronize on both sides, max
+over ranks).  `e2e` repeats the headline form through the public API with
+host buffers: the initial fields are uploaded from pinned host memory, every
+step returns its telemetry to the host (as FluidSolver3D::step does), and the
+final density/temperature hand-off (FluidMedium::from_solver) is downloaded.
+
+`--impl reference` times the CPU oracle (a C++ restatement of the reference's
+single-threaded Rust solver; the Rust crate cannot be built in this image) on
+a bounded sample of the same workload in f64.
+
+Multi-GPU: the single simulation does not shard; N ranks run N independent
+replicas (weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "aether-core-engine_b200"))
+
+METRIC = ("Mcell-steps/s 128³: FP32+FP64-refine vs FP64 GPU @1e-5 err; "
+          "adjoint/fwd ratio")
+UNIT = "Mcell-steps/s"
+WORKLOAD = "smoke plume 128x128x128, sphere source r=10 at (64,12.8,64), seed 0, dt=0.5h"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=128, help="grid edge (default 128)")
+    ap.add_argument("--forms", default="mixed_cg,fp64_cg,fp64_sor,mixed_sor")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0,
+                    help="target length of the bounded CPU sample")
+    return ap.parse_args()
+
+
+def plume_for(form: str, n: int):
+    from aether_fluid.plume import Plume
+    if form.endswith("sor"):
+        return Plume(n, n, n, 200, seed=0, solver="sor", iters=80)
+    return Plume(n, n, n, 200, seed=0)
+
+
+# ---------------------------------------------------------------- clocks -----
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    QUERY = ("pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str | None):
+        self.bus_id = (bus_id or "").lower()
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        rows = self.rows
+        if self.bus_id:
+            mine = [r for r in rows if r[0].lower().endswith(self.bus_id[-12:])]
+            rows = mine or rows
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------ byte model -----
+def poisson_bytes(n_cells: int, form: str, infos) -> float:
+    """Algorithmic bytes of the Poisson kernel over the given solves: per cell,
+    f64 CG 32 (init) + 88 per iteration; mixed CG 52 per refinement pass + 44
+    per inner iteration; SOR 24 per sweep (f64) / 12 (f32) plus, for the mixed
+    form, 52 for its one f64 residual/correction pass."""
+    total = 0.0
+    for inf in infos:
+        if form == "fp64_cg":
+            total += 32 + 88 * inf.iterations
+        elif form == "mixed_cg":
+            total += 52 * max(inf.refinements, 1) + 44 * inf.iterations
+        elif form == "fp64_sor":
+            total += 24 * inf.iterations
+        else:
+            total += 52 + 12 * inf.iterations
+    return total * n_cells
+
+
+def step_bytes(n_cells: int, form: str, infos) -> float:
+    """Whole-step algorithmic bytes: f64 CG 336 + 88*N_it, f64 SOR 304 + 24*S,
+    mixed CG 160 + 52*R + 44*N_in, mixed SOR 160 + 52 + 12*S."""
+    total = 0.0
+    for inf in infos:
+        if form == "fp64_cg":
+            total += 336 + 88 * inf.iterations
+        elif form == "fp64_sor":
+            total += 304 + 24 * inf.iterations
+        elif form == "mixed_cg":
+            total += 160 + 52 * max(inf.refinements, 1) + 44 * inf.iterations
+        else:
+            total += 160 + 52 + 12 * inf.iterations
+    return total * n_cells
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- our arm ----
+def time_form(form: str, n: int, steps: int, warmup: int, dist, torch, rank: int):
+    import aether_fluid as af
+    p = plume_for(form, n)
+    s = p.build(precision=af.Precision.MIXED if form.startswith("mixed") else af.Precision.FP64)
+    if warmup > 0:
+        s.run(warmup, p.dt, 0.0, p.dt)
+    s.init_velocity_noise(p.seed)  # back to the initial state, outside the timed region
+    stream = torch.cuda.ExternalStream(s.stream)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    s.set_stage_timing(True)
+    launches0 = s.launch_count()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start.record(stream)
+    tel, infos = s.run(steps, p.dt, 0.0, p.dt)
+    end.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    launches = s.launch_count() - launches0
+    stages = s.stage_timing()
+    s.set_stage_timing(False)
+    fields = {f: s.get_field(f) for f in ("u", "v", "w", "density", "temperature")}
+    s.close()
+    return {"ms": ms, "infos": infos, "tel": tel, "stages": stages, "launches": launches,
+            "fields": fields, "cells": p.cells}
+
+
+def time_e2e(form: str, n: int, steps: int, warmup: int, dist, torch):
+    """Headline form through the public API with host buffers."""
+    import aether_fluid as af
+    from aether_fluid import _lib
+    p = plume_for(form, n)
+    s = p.build(precision=af.Precision.MIXED if form.startswith("mixed") else af.Precision.FP64)
+    # The initial condition, generated once on the host into pinned memory.
+    s.init_velocity_noise(p.seed)
+    init = {f: torch.empty(p.cells, dtype=torch.float64, pin_memory=True)
+            for f in ("u", "v", "w")}
+    for f, t in init.items():
+        t.numpy()[:] = s.get_field(f)
+    out_d = torch.empty(p.cells, dtype=torch.float64, pin_memory=True)
+    out_t = torch.empty(p.cells, dtype=torch.float64, pin_memory=True)
+    lib = _lib.load()
+    dp = ctypes.POINTER(ctypes.c_double)
+
+    def one_run(k):
+        # host -> device: the step inputs (initial velocity) from pinned memory
+        for fid, f in enumerate(("u", "v", "w")):
+            _lib.check(lib.afl_upload_field(s._h, fid, ctypes.cast(init[f].data_ptr(), dp),
+                                            p.cells))
+        tel = [s.step(p.dt, step * p.dt) for step in range(k)]  # telemetry per step
+        mx = ctypes.c_double()
+        _lib.check(lib.afl_medium_handoff(s._h, ctypes.cast(out_d.data_ptr(), dp),
+                                          ctypes.cast(out_t.data_ptr(), dp), p.cells,
+                                          ctypes.byref(mx)))
+        return tel
+
+    one_run(warmup)                      # warm-up pass
+    s.init_velocity_noise(p.seed)        # reset density/temperature/pressure (untimed)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    one_run(steps)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([el], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el = float(t.item())
+    s.close()
+    h2d = 3 * p.cells * 8
+    d2h = steps * 64 + 2 * p.cells * 8 + 8
+    return {"seconds": el, "h2d_per_step": h2d / steps, "d2h_per_step": d2h / steps}
+
+
+def cpu_sample(n: int, seconds: float):
+    """The oracle (f64, 1 thread) on the first steps of the same plume until
+    `seconds` of CPU time have been spent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    p = plume_for("fp64_cg", n)
+    s = O.OracleSolver(p.nx, p.ny, p.nz)
+    s.set_params(vorticity_eps=p.eps, buoyancy_beta=p.beta, gravity_alpha=p.alpha,
+                 solver_kind=O.CG, solver_iters=p.iters, cg_rel_tol=p.rel_tol)
+    s.init_velocity_noise(p.seed)
+    s.set_sphere_source(p.center, p.radius)
+    t0 = time.perf_counter()
+    steps, iters = 0, []
+    while True:
+        s.step(p.dt, steps * p.dt)
+        iters.append(s.last_cg_iters())
+        steps += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    el = time.perf_counter() - t0
+    return {"value": p.cells * steps / el / 1e6, "steps": steps, "seconds": el,
+            "cg_iters": iters}
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_ours(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as tdist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist = tdist
+    else:
+        torch.cuda.set_device(local)
+    import aether_fluid as af
+    af.load()
+
+    forms = [f for f in args.forms.split(",") if f]
+    headline = forms[0]
+    props = torch.cuda.get_device_properties(local)
+    bus = getattr(props, "pci_bus_id", None)
+    results = {}
+    clocks = None
+    for form in forms:
+        sampler = ClockSampler(bus) if form == headline else None
+        if sampler:
+            sampler.start()
+        r = time_form(form, args.n, args.steps, args.warmup, dist, torch, rank)
+        if sampler:
+            clocks = sampler.stop()
+        ms = r["ms"]
+        if dist:
+            t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        r["ms_max"] = ms
+        results[form] = r
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = time_e2e(headline, args.n, args.steps, args.warmup, dist, torch)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(args.n, args.cpu_seconds)
+
+    if rank == 0:
+        import numpy as np
+        head = results[headline]
+        cells = head["cells"]
+        value = cells * args.steps * world / (head["ms_max"] / 1e3) / 1e6
+        peak, peak_kind = measured_peak()
+        pois_ms, pois_calls = head["stages"]["poisson"]
+        pois_bytes = poisson_bytes(cells, headline, head["infos"])
+        achieved = pois_bytes / pois_calls / (pois_ms / pois_calls / 1e3) / 1e9
+        variants = {}
+        for form, r in results.items():
+            its = [i.iterations for i in r["infos"]]
+            sb = step_bytes(cells, form, r["infos"])
+            variants[form] = {
+                "value": cells * args.steps * world / (r["ms_max"] / 1e3) / 1e6,
+                "ms_per_step": r["ms_max"] / args.steps,
+                "mean_solver_iters": float(np.mean(its)),
+                "max_solver_iters": int(np.max(its)),
+                "converged_steps": int(sum(i.converged for i in r["infos"])),
+                "step_roofline_frac": sb / (r["ms"] / 1e3) / 1e9 / peak,
+                "stage_ms": {k: round(v[0], 3) for k, v in r["stages"].items()},
+            }
+        # accuracy of the mixed forms against the f64 GPU forms after K steps
+        for mixed, ref in (("mixed_cg", "fp64_cg"), ("mixed_sor", "fp64_sor")):
+            if mixed in results and ref in results:
+                errs = {}
+                for f, a in results[mixed]["fields"].items():
+                    b = results[ref]["fields"][f]
+                    den = float(np.linalg.norm(b))
+                    errs[f] = float(np.linalg.norm(a - b) / den) if den > 0 else 0.0
+                variants[mixed]["rel_l2_vs_" + ref] = errs
+        if "mixed_cg" in variants and "fp64_cg" in variants:
+            variants["mixed_cg"]["speedup_vs_fp64_cg"] = (
+                variants["mixed_cg"]["value"] / variants["fp64_cg"]["value"])
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": head["ms_max"] / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32+f64" if headline.startswith("mixed") else "f64",
+            "data": "synthetic (seeded velocity noise, sphere source)",
+            "config": {"workload": WORKLOAD, "form": headline, "grid": [args.n] * 3,
+                       "solver": "CG rel 1e-6 max 200" if "cg" in headline else
+                       "RB-SOR omega 1.7 x 80", "parallelism": f"replicas x{world}",
+                       "l2": "state larger than L2 (no flush between steps)"},
+            "gpu_launches": int(head["launches"]),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "k_cg_mixed" if headline == "mixed_cg" else headline,
+                         "peak_source": peak_kind},
+            "variants": variants,
+            "adjoint_fwd_ratio": None,
+        }
+        if e2e:
+            line["e2e"] = {"value": cells * args.steps * world / e2e["seconds"] / 1e6,
+                           "unit": UNIT, "h2d_bytes_per_step": e2e["h2d_per_step"],
+                           "d2h_bytes_per_step": e2e["d2h_per_step"]}
+        if cpu:
+            line["cpu_baseline"] = {
+                "value": cpu["value"], "unit": UNIT, "cores": 1, "kind": "port",
+                "sample": (f"first {cpu['steps']} steps of the same plume in f64 "
+                           f"(CG iters {cpu['cg_iters']}), {cpu['seconds']:.1f} s on "
+                           f"{cpu_model()}")}
+        line["clocks"] = clocks
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    warm = min(args.warmup, 1)
+    budget = max(args.cpu_seconds, 10.0)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    p = plume_for("fp64_cg", args.n)
+    s = O.OracleSolver(p.nx, p.ny, p.nz)
+    s.set_params(vorticity_eps=p.eps, buoyancy_beta=p.beta, gravity_alpha=p.alpha,
+                 solver_kind=O.CG, solver_iters=p.iters, cg_rel_tol=p.rel_tol)
+    s.init_velocity_noise(p.seed)
+    s.set_sphere_source(p.center, p.radius)
+    for n in range(warm):
+        s.step(p.dt, n * p.dt)
+    t0 = time.perf_counter()
+    steps, iters = 0, []
+    while steps < args.steps:
+        s.step(p.dt, (warm + steps) * p.dt)
+        iters.append(s.last_cg_iters())
+        steps += 1
+        if time.perf_counter() - t0 >= budget:
+            break
+    el = time.perf_counter() - t0
+    value = p.cells * steps / el / 1e6
+    sample = (f"steps {warm}..{warm + steps - 1} of the 128^3 plume in f64 on 1 core "
+              f"(CG iters {iters}); C++ restatement of the reference's single-threaded "
+              f"Rust solver (no Rust toolchain here), {cpu_model()}")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+        "steps": steps, "warmup": warm, "ms_per_step": el * 1e3 / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded velocity noise, sphere source)",
+        "config": {"workload": WORKLOAD, "form": "reference f64 CG", "grid": [args.n] * 3},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,213 @@
+"""Whole-step parity of the CUDA path: the reference's own known answer and
+invariant tests run through the C ABI, the committed golden fixtures, the
+64^3 x 50 smoke plume against the live oracle, determinism, and the error
+paths (bounded barrier waits, non-finite residuals)."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_DIR, ROOT
+from helpers import oracle_for, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("u", "v", "w", "density", "temperature", "pressure")
+
+
+def load_golden(name):
+    return np.load(os.path.join(GOLDEN_DIR, f"{name}.npz"))
+
+
+def test_readme_known_answer(af):
+    """README.md:54 / src/verify.rs:229-250 through the C ABI."""
+    s = af.FluidSolver3D(16, 20, 16)
+    s.set_params(solver_kind=0, solver_iters=40)
+    s.inject_cyberpunk_sources(0.5, 0.1)
+    s.apply_buoyancy_and_vorticity_confinement(0.1)
+    pre = s.compute_divergence_norm()
+    info = s.project()
+    post = s.compute_divergence_norm()
+    assert f"{pre:.4e}" == "2.5751e+00"
+    assert f"{post:.4e}" == "6.7289e-03"
+    assert post <= 0.03 * pre
+    gold = load_golden("verify_check4")
+    assert info.iterations == int(gold["cg_iters"])
+    for f in FIELDS:
+        assert rel_l2(s.get_field(f), gold[f]) <= 1e-11, f
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_burst_projection(af, kind):
+    """src/fluid.rs:918-956 through the C ABI, against the golden fields."""
+    s = af.FluidSolver3D(18, 22, 18)
+    s.set_params(solver_kind=kind, solver_iters=45 if kind == 0 else 90)
+    u, v, w = s.u, s.v, s.w
+    for k in range(6, 12):
+        for j in range(5, 11):
+            for i in range(6, 12):
+                c = s.idx(i, j, k)
+                u[c] = (i - 8.5) * 3.0
+                v[c] = (j - 7.5) * 4.5
+                w[c] = (k - 8.5) * 2.5
+    s.u, s.v, s.w = u, v, w
+    s.enforce_wall_velocity_bc()
+    before = s.compute_divergence_norm()
+    assert before > 1.0
+    s.project()
+    after = s.compute_divergence_norm()
+    assert after < before * 0.02
+    gold = load_golden("burst_cg" if kind == 0 else "burst_rbgs")
+    for f in FIELDS:
+        got = s.get_field(f)
+        if kind == 1:  # RB-SOR has no reduction: bit exact
+            assert np.array_equal(got, gold[f]), f
+        else:
+            assert rel_l2(got, gold[f]) <= 1e-11, f
+
+
+def test_two_steps_positivity(af):
+    """src/fluid.rs:959-968 (cyberpunk jets, reference defaults)."""
+    s = af.FluidSolver3D(16, 20, 16)
+    f1 = s.step(0.08, 0.2)
+    f2 = s.step(0.08, 0.4)
+    assert f1.kinetic_energy > 0.0 and f2.enstrophy > 0.0
+    d = s.density
+    assert np.all(np.isfinite(d)) and np.all(d >= 0.0)
+    gold = load_golden("two_steps")
+    np.testing.assert_allclose(np.stack([f1.as_array(), f2.as_array()]), gold["telemetry"],
+                               rtol=1e-9)
+    for f in FIELDS:
+        assert rel_l2(s.get_field(f), gold[f]) <= 1e-9, f
+
+
+@pytest.mark.parametrize("name", ["plume_cg_24x20x18", "plume_sor_20x24x16"])
+def test_plume_fixtures(af, name):
+    from golden.gen_golden import PLUME_CG, PLUME_SOR
+    p = PLUME_CG if "cg" in name else PLUME_SOR
+    gold = load_golden(name)
+    s = p.build()
+    tel, infos = s.run(p.steps, p.dt, 0.0, p.dt)
+    if p.solver == "cg":
+        its = np.array([i.iterations for i in infos])
+        assert np.all(np.abs(its - gold["cg_iters"]) <= 1), (its, gold["cg_iters"])
+    np.testing.assert_allclose(tel, gold["telemetry"], rtol=1e-8, atol=1e-300)
+    for f in FIELDS:
+        assert rel_l2(s.get_field(f), gold[f]) <= 1e-8, f
+
+
+def test_config_64cube_fp64_parity(af, oracle):
+    """The 64^3 x 50-step plume (seed 0, CG to 1e-6) after the last step:
+    every field within 1e-5 relative L2 of the f64 oracle."""
+    from aether_fluid.plume import Plume
+    p = Plume(64, 64, 64, 50, seed=0)
+    o = oracle_for(p, oracle)
+    otel, _ = o.run(p.steps, p.dt, 0.0, p.dt, telemetry=True), None
+    s = p.build()
+    tel, infos = s.run(p.steps, p.dt, 0.0, p.dt)
+    for f in ("u", "v", "w", "density", "temperature"):
+        err = rel_l2(s.get_field(f), o.field(f))
+        assert err <= 1e-5, (f, err)
+    ref_tel = otel[0][1] if isinstance(otel[0], tuple) else otel[1]
+    np.testing.assert_allclose(tel[:, 1:5], ref_tel[:, 1:5], rtol=1e-5)
+
+
+def test_config_64cube_mixed_parity(af, oracle):
+    """Same plume in the mixed form: within 1e-4 relative L2 of the f64 oracle."""
+    from aether_fluid.plume import Plume
+    p = Plume(64, 64, 64, 50, seed=0)
+    o = oracle_for(p, oracle)
+    o.run(p.steps, p.dt, 0.0, p.dt)
+    s = p.build(precision=1)
+    _, infos = s.run(p.steps, p.dt, 0.0, p.dt)
+    for f in ("u", "v", "w", "density", "temperature"):
+        err = rel_l2(s.get_field(f), o.field(f))
+        assert err <= 1e-4, (f, err)
+
+
+def test_sor_plume_fp64_bit_exact_short(af, oracle):
+    """RB-SOR omega=1.7 plume, 3 steps at 40x36x32: every stage of the step is
+    fixed-order arithmetic except telemetry, so the fields match bit for bit."""
+    from aether_fluid.plume import Plume
+    p = Plume(40, 36, 32, 3, seed=5, solver="sor", iters=80)
+    o = oracle_for(p, oracle)
+    o.run(p.steps, p.dt, 0.0, p.dt)
+    s = p.build()
+    s.run(p.steps, p.dt, 0.0, p.dt)
+    for f in FIELDS:
+        assert np.array_equal(s.get_field(f), o.field(f)), f
+
+
+def test_run_matches_step_and_is_deterministic(af):
+    from aether_fluid.plume import Plume
+    p = Plume(32, 40, 28, 6, seed=9)
+    a = p.build()
+    ta, _ = a.run(p.steps, p.dt, 0.0, p.dt)
+    b = p.build()
+    tb = np.stack([b.step(p.dt, n * p.dt).as_array() for n in range(p.steps)])
+    assert np.array_equal(ta, tb)
+    for f in FIELDS:
+        assert np.array_equal(a.get_field(f), b.get_field(f)), f
+
+
+@pytest.mark.parametrize("n", [96, 128])
+def test_large_grid_properties(af, n):
+    """Size-independent properties at full sizes: projection removes the
+    divergence, density stays non-negative and finite, mass is positive."""
+    from aether_fluid.plume import Plume
+    for precision in (0, 1):
+        p = Plume(n, n, n, 3, seed=1)
+        s = p.build(precision=precision)
+        tel, infos = s.run(p.steps, p.dt, 0.0, p.dt)
+        assert all(i.converged for i in infos), infos
+        assert s.compute_divergence_norm() < 1e-3
+        d = s.density
+        assert np.all(np.isfinite(d)) and d.min() >= 0.0 and tel[-1, 4] > 0
+
+
+def test_barrier_timeout_is_reported_not_hung(af):
+    """A persistent kernel whose barrier wait limit runs out returns
+    AFL_ERR_TIMEOUT; the context stays usable.  The limit is set to 0 ns by the
+    host (no GPU fault, no endless wait)."""
+    code = r"""
+import os, sys
+sys.path.insert(0, os.path.join(sys.argv[1], "aether-core-engine_b200"))
+os.environ["AFL_BARRIER_TIMEOUT_NS"] = "0"
+import aether_fluid as af
+s = af.FluidSolver3D(64, 64, 64)
+s.set_field("divergence", __import__("numpy").random.default_rng(0).standard_normal(s.n))
+try:
+    s.solve_poisson_conjugate_gradient(50)
+    print("NO-ERROR")
+except af.AetherFluidError as e:
+    print("STATUS", e.status)
+os.environ.pop("AFL_BARRIER_TIMEOUT_NS")
+t = af.FluidSolver3D(16, 20, 16)
+print("STEP-OK", t.step(0.08, 0.2).kinetic_energy > 0)
+"""
+    out = subprocess.run([sys.executable, "-c", code, ROOT], capture_output=True, text=True,
+                         timeout=120)
+    assert "STATUS 5" in out.stdout, out.stdout + out.stderr
+    assert "STEP-OK True" in out.stdout, out.stdout + out.stderr
+
+
+def test_nonfinite_residual_reported(af):
+    s = af.FluidSolver3D(20, 20, 20)
+    b = np.zeros(s.n)
+    b[s.idx(10, 10, 10)] = np.nan
+    s.set_field("divergence", b)
+    with pytest.raises(af.AetherFluidError) as e:
+        s.solve_poisson_conjugate_gradient(10)
+    assert e.value.status == 4
+    # the handle keeps working afterwards
+    s.set_field("divergence", np.zeros(s.n))
+    s.solve_poisson_conjugate_gradient(10)
+
+
+def test_invalid_field_length(af):
+    s = af.FluidSolver3D(8, 8, 8)
+    with pytest.raises(af.AetherFluidError) as e:
+        s.set_field("u", np.zeros(10))
+    assert e.value.status == 1
