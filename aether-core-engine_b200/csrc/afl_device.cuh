@@ -230,7 +230,7 @@ __device__ inline bool grid_sync(const GridSync &gs) {
       unsigned int spins = 0;
       while (ld_acquire(gs.gen) == g0) {
         if (ld_relaxed_i32(gs.abort_flag) != 0) { ok = 0; break; }
-        if ((++spins & 63u) == 0 && global_ns() - t0 > gs.timeout_ns) {
+        if ((spins++ & 15u) == 0 && global_ns() - t0 > gs.timeout_ns) {
           atomicCAS(gs.abort_flag, 0, 1);
           ok = 0;
           break;

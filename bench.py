@@ -114,7 +114,7 @@ class ClockSampler:
             self.thread.join(timeout=5)
         rows = self.rows
         if self.bus_id:
-            mine = [r for r in rows if r[0].lower().endswith(self.bus_id[-12:])]
+            mine = [r for r in rows if r[0].lower().startswith(self.bus_id)]
             rows = mine or rows
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
@@ -306,7 +306,10 @@ def run_ours(args):
     forms = [f for f in args.forms.split(",") if f]
     headline = forms[0]
     props = torch.cuda.get_device_properties(local)
-    bus = getattr(props, "pci_bus_id", None)
+    try:
+        bus = f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}"
+    except AttributeError:
+        bus = None
     results = {}
     clocks = None
     for form in forms:

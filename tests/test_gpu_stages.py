@@ -20,13 +20,21 @@ VEL = ("u", "v", "w")
 SCAL = ("density", "temperature")
 
 
-def seeded_state(n, seed, vel_scale):
+def seeded_state(shape, seed, vel_scale):
+    nx, ny, nz = shape
+    n = nx * ny * nz
     rng = np.random.default_rng(seed)
     st = {f: rng.uniform(-vel_scale, vel_scale, n) for f in VEL}
     st["density"] = rng.uniform(0.0, 2.0, n)
     st["temperature"] = rng.uniform(0.0, 1.5, n)
     st["pressure"] = rng.standard_normal(n) * 0.01
-    st["divergence"] = rng.standard_normal(n) * 0.01
+    # A right-hand side the singular Neumann operator can match: zero off the
+    # interior and zero-mean on it (a divergence field of walled velocities
+    # has both properties).
+    b = np.zeros((nz, ny, nx))
+    inner = rng.standard_normal((nz - 2, ny - 2, nx - 2)) * 0.01
+    b[1:-1, 1:-1, 1:-1] = inner - inner.mean()
+    st["divergence"] = b.ravel()
     return st
 
 
@@ -37,7 +45,7 @@ def pair(af, O, shape, seed=0, vel_scale=1.0, precision=0, **params):
     if params:
         g.set_params(**params)
         o.set_params(**{k: v for k, v in params.items() if k != "source_kind"})
-    st = seeded_state(g.n, seed, vel_scale)
+    st = seeded_state(shape, seed, vel_scale)
     for f, vals in st.items():
         g.set_field(f, vals)
         o.field(f)[:] = vals
