@@ -48,7 +48,7 @@ class AflParams(ctypes.Structure):
         ("mixed_inner_iters", ctypes.c_int32),
         ("mixed_inner_rel_tol", ctypes.c_double),
         ("mixed_max_refinements", ctypes.c_int32),
-        ("reserved_i32", ctypes.c_int32),
+        ("poisson_kernel", ctypes.c_int32),
         ("reserved_f64", ctypes.c_double * 4),
     ]
 
@@ -126,6 +126,7 @@ SIGNATURES = [
     ("afl_sample_trilinear", _st, [_vp, _i, _dp, _sz, _dp]),
     ("afl_set_stage_timing", _st, [_vp, _i]),
     ("afl_get_stage_timing", _st, [_vp, _dp, ctypes.POINTER(ctypes.c_int64)]),
+    ("afl_get_poisson_plan", _st, [_vp, ctypes.POINTER(ctypes.c_int32)]),
     ("afl_get_launch_count", _st, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     ("afl_synchronize", _st, [_vp]),
     ("afl_stream", _vp, [_vp]),

@@ -85,7 +85,7 @@ class FluidSolver3D:
     _KNOBS = ("vorticity_eps", "buoyancy_beta", "gravity_alpha", "solver_iters",
               "sor_omega", "cg_rel_tol", "sphere_radius", "sphere_density",
               "sphere_temperature", "fail_on_not_converged", "mixed_inner_iters",
-              "mixed_inner_rel_tol", "mixed_max_refinements")
+              "mixed_inner_rel_tol", "mixed_max_refinements", "poisson_kernel")
 
     def __init__(self, nx: int, ny: int, nz: int, precision: Precision = Precision.FP64,
                  **params):
@@ -290,6 +290,12 @@ class FluidSolver3D:
         calls = (ctypes.c_int64 * n)()
         check(self._lib.afl_get_stage_timing(self._h, ms, calls))
         return {name: (ms[i], calls[i]) for i, name in enumerate(_lib.STAGES)}
+
+    def poisson_plan(self) -> dict:
+        out = (ctypes.c_int32 * 4)()
+        check(self._lib.afl_get_poisson_plan(self._h, out))
+        return {"resident": bool(out[0]), "tile": (16, out[1]), "cells_per_thread": out[2],
+                "ctas": out[3]}
 
     def launch_count(self) -> int:
         out = ctypes.c_uint64()

@@ -132,6 +132,35 @@ struct SorMixedArgs {
 };
 int launch_rbsor_mixed(const SorMixedArgs &a, const PersistentState &ps, cudaStream_t st);
 
+// On-chip resident CG (afl_poisson_resident.cu): one 1024-thread CTA per SM
+// owns a 16 x ty column tile spanning all z planes.
+struct ResidentPlan {
+  int ty;          // tile height in y (cells)
+  int cpt;         // z cells per thread
+  int tiles_x, tiles_y;
+  int smem_bytes;  // dynamic shared memory per CTA
+};
+struct ResidentCgArgs {
+  Dims g;
+  int tiles_x, tiles_y;
+  double *p;            // f64 pressure
+  const double *b;      // f64 right-hand side
+  void *rpub;           // published tile-edge residual (f64 or f32, n cells)
+  void *dpub0, *dpub1;  // published tile-edge direction, by iteration parity
+  int max_iters;        // FP64: CG iterations; mixed: inner iterations, all passes
+  int max_inner;        // mixed: inner iterations per refinement pass
+  int max_refine;       // mixed: refinement passes
+  double inner_rel_tol; // mixed
+  double rel_tol;
+  SolveReport *report;
+};
+// False when the grid does not fit on chip (too many tiles, too much shared
+// memory, or more than 16 z cells per thread).
+bool plan_resident(const Dims &g, bool f64, ResidentPlan *plan);
+size_t resident_smem_bytes(const Dims &g, int ty, bool f64);
+int launch_cg_resident(const ResidentCgArgs &a, const ResidentPlan &plan, bool f64,
+                       const PersistentState &ps, cudaStream_t st);
+
 // Occupancy-derived CTA count of each persistent kernel (co-residency bound).
 int persistent_blocks_cg_f64();
 int persistent_blocks_sor_f64();

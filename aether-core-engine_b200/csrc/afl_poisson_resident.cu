@@ -1,0 +1,523 @@
+// afl_poisson_resident.cu -- on-chip resident CG solves for grids that fit.
+//
+// One 1024-thread CTA per SM owns a column tile of 16 x TY cells in x-y that
+// spans every z plane.  During the solve nothing of the tile leaves the SM:
+//   * the search direction d lives in shared memory (tile + one-cell halo
+//     ring in x and y), because the 7-point operator reads it at neighbours;
+//   * the residual r (and, in the mixed form, the f32 correction e) live in
+//     registers, CPT consecutive z cells per thread.
+// Per iteration only the tile-edge values cross L2: each CTA publishes the
+// r and d of its edge cells, and rebuilds its halo ring from its neighbours'
+// published values.  The direction update d = r + beta*d (src/fluid.rs:483-485)
+// is evaluated for halo cells from the neighbours' published r and previous d
+// with the same expression the owner uses, so halo and owner agree bit for bit
+// and an iteration needs two grid barriers, as in the streaming kernel.
+//
+// Built with -fmad=false: the FP64 kernel keeps the reference's un-fused
+// arithmetic; the mixed kernel writes its FMAs explicitly (__fmaf_rn), so
+// owner and halo evaluate identical operations.
+#include "afl_launch.h"
+
+namespace afl {
+namespace {
+
+constexpr int kRT = 1024;       // threads per CTA
+constexpr int kRW = kRT / 32;   // warps per CTA
+constexpr int kTX = 16;         // tile width in x (cells)
+
+template <int NV>
+__device__ __forceinline__ void bsum(double (&v)[NV], double *scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < NV; ++a) v[a] = warp_sum(v[a]);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int a = 0; a < NV; ++a) scratch[warp * NV + a] = v[a];
+  __syncthreads();
+#pragma unroll
+  for (int a = 0; a < NV; ++a) {
+    double s = 0.0;
+    for (int w = 0; w < kRW; ++w) s += scratch[w * NV + a];
+    v[a] = s;
+  }
+  __syncthreads();
+}
+
+// Fixed-order sum of NV interleaved per-CTA partials; identical in every CTA.
+template <int NV>
+__device__ __forceinline__ void reduce_parts(const double *parts, int nparts,
+                                             double (&out)[NV], double *scratch) {
+#pragma unroll
+  for (int a = 0; a < NV; ++a) out[a] = 0.0;
+  for (int b = threadIdx.x; b < nparts; b += kRT)
+#pragma unroll
+    for (int a = 0; a < NV; ++a) out[a] += __ldcg(parts + b * NV + a);
+  bsum<NV>(out, scratch);
+}
+
+template <int NV>
+__device__ __forceinline__ void publish(double *parts, const double (&v)[NV]) {
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int a = 0; a < NV; ++a) parts[blockIdx.x * NV + a] = v[a];
+}
+
+// Where this thread's cells sit: column (ii, jj) of the tile, planes
+// k0 .. k0+CPT-1.
+template <int TY, int CPT>
+struct Cells {
+  static constexpr int kCols = kTX * TY;
+  static_assert(kRT % kCols == 0, "a CTA must cover whole column groups");
+  static constexpr int SX = kTX + 2;
+  static constexpr int SXY = (kTX + 2) * (TY + 2);
+  int i, j, k0;
+  int c0, s0;        // global / shared index of plane k0
+  bool in_ij;        // column inside the grid
+  bool ij_interior;  // 1 <= i <= nx-2 and 1 <= j <= ny-2
+  bool edge;         // value needed by a neighbouring tile
+  __device__ Cells(const Dims &g, int tiles_x) {
+    const int t = threadIdx.x;
+    const int col = t % kCols, grp = t / kCols;
+    const int ii = col % kTX, jj = col / kTX;
+    const int bx = blockIdx.x % tiles_x, by = blockIdx.x / tiles_x;
+    i = bx * kTX + ii;
+    j = by * TY + jj;
+    k0 = grp * CPT;
+    in_ij = i < g.nx && j < g.ny;
+    ij_interior = i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2;
+    edge = ii == 0 || ii == kTX - 1 || jj == 0 || jj == TY - 1;
+    c0 = (k0 * g.ny + j) * g.nx + i;
+    s0 = (k0 * (TY + 2) + jj + 1) * SX + ii + 1;
+  }
+  __device__ bool valid(const Dims &g, int m) const { return in_ij && k0 + m < g.nz; }
+  __device__ bool interior(const Dims &g, int m) const {
+    const int k = k0 + m;
+    return ij_interior && k >= 1 && k <= g.nz - 2;
+  }
+};
+
+// The reference operator (src/fluid.rs:356-394) on the shared-memory tile.
+template <typename R, int SX, int SXY>
+__device__ __forceinline__ R lap_smem(const Dims &g, const R *D, int s, int i, int j, int k) {
+  R diag = R(0), nb = R(0);
+  if (i > 1) { diag += R(1); nb += D[s - 1]; }
+  if (i + 2 < g.nx) { diag += R(1); nb += D[s + 1]; }
+  if (j > 1) { diag += R(1); nb += D[s - SX]; }
+  if (j + 2 < g.ny) { diag += R(1); nb += D[s + SX]; }
+  if (k > 1) { diag += R(1); nb += D[s - SXY]; }
+  if (k + 2 < g.nz) { diag += R(1); nb += D[s + SXY]; }
+  return diag * D[s] - nb;
+}
+
+// The same operator on the f64 pressure in global memory.
+__device__ __forceinline__ double lap_global(const Dims &g, const double *x, int c, int i, int j,
+                                             int k) {
+  double diag = 0.0, nb = 0.0;
+  if (i > 1) { diag += 1.0; nb += x[c - 1]; }
+  if (i + 2 < g.nx) { diag += 1.0; nb += x[c + 1]; }
+  if (j > 1) { diag += 1.0; nb += x[c - g.nx]; }
+  if (j + 2 < g.ny) { diag += 1.0; nb += x[c + g.nx]; }
+  if (k > 1) { diag += 1.0; nb += x[c - g.nxy]; }
+  if (k + 2 < g.nz) { diag += 1.0; nb += x[c + g.nxy]; }
+  return diag * x[c] - nb;
+}
+
+// Rebuilds the halo ring (x and y neighbours of the tile, every plane) from
+// the neighbours' published values: dn = r (first iteration) or dn = f(r, d).
+template <typename R, int TY, typename F>
+__device__ __forceinline__ void fill_halo(const Dims &g, int tiles_x, R *D, const F &value_at) {
+  constexpr int SX = kTX + 2;
+  constexpr int per_plane = 2 * TY + 2 * kTX;
+  const int bx = blockIdx.x % tiles_x, by = blockIdx.x / tiles_x;
+  const int total = per_plane * g.nz;
+  for (int h = threadIdx.x; h < total; h += kRT) {
+    const int k = h / per_plane;
+    const int q = h - k * per_plane;
+    int ii, jj;
+    if (q < TY) { ii = -1; jj = q; }
+    else if (q < 2 * TY) { ii = kTX; jj = q - TY; }
+    else if (q < 2 * TY + kTX) { ii = q - 2 * TY; jj = -1; }
+    else { ii = q - 2 * TY - kTX; jj = TY; }
+    const int i = bx * kTX + ii, j = by * TY + jj;
+    const int s = (k * (TY + 2) + jj + 1) * SX + ii + 1;
+    R v = R(0);
+    if (i >= 0 && i < g.nx && j >= 0 && j < g.ny) v = value_at((k * g.ny + j) * g.nx + i);
+    D[s] = v;
+  }
+}
+
+struct Ring2 {
+  double *base;
+  int stride;
+  __device__ double *buf(int phase) const { return base + (phase & 1) * stride; }
+};
+
+// ---------------------------------------------------------------- FP64 ------
+// solve_poisson_conjugate_gradient (src/fluid.rs:445-493) with the relative
+// tolerance extension; p stays in global memory (updated once per iteration).
+template <int TY, int CPT>
+__global__ void __launch_bounds__(kRT, 1)
+    k_cg_res_f64(ResidentCgArgs a, GridSync gs, Ring2 pr) {
+  using C = Cells<TY, CPT>;
+  extern __shared__ double D[];
+  __shared__ double scratch[kRW * 2];
+  const Dims g = a.g;
+  const C cl(g, a.tiles_x);
+  double *p = a.p;
+  const double *b = a.b;
+  double *rpub = static_cast<double *>(a.rpub);
+  double *dpub[2] = {static_cast<double *>(a.dpub0), static_cast<double *>(a.dpub1)};
+  double r[CPT];
+  int phase = 0;
+  {
+    double acc[2] = {0.0, 0.0};
+#pragma unroll
+    for (int m = 0; m < CPT; ++m) {
+      r[m] = 0.0;
+      if (!cl.valid(g, m)) continue;
+      const int c = cl.c0 + m * g.nxy;
+      const double ap = cl.interior(g, m) ? lap_global(g, p, c, cl.i, cl.j, cl.k0 + m) : 0.0;
+      const double bc = __ldg(b + c);
+      const double rv = bc - ap;
+      r[m] = rv;
+      if (cl.edge) rpub[c] = rv;
+      acc[0] += rv * rv;
+      acc[1] += bc * bc;
+    }
+    bsum<2>(acc, scratch);
+    publish<2>(pr.buf(phase), acc);
+  }
+  if (!grid_sync(gs)) return;
+  double tot[2];
+  reduce_parts<2>(pr.buf(phase), gridDim.x, tot, scratch);
+  ++phase;
+  double delta = tot[0];
+  const double bb = tot[1];
+  double tol2 = -1.0;
+  if (a.rel_tol > 0.0) {
+    const double tl = a.rel_tol * sqrt(bb);
+    tol2 = tl * tl;
+  }
+  const double delta0 = delta;
+  double last = delta;
+  int it = 0, converged = 0, par = 0;
+  if (!(delta > 1e-24) || (tol2 >= 0.0 && delta <= tol2)) {
+    converged = isfinite(delta) ? 1 : 0;
+  } else {
+    double beta = 0.0;
+    while (it < a.max_iters) {
+      const bool first = it == 0;
+      // d = r + beta*d on the tile, published for the neighbours
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) {
+        if (!cl.valid(g, m)) continue;
+        const int s = cl.s0 + m * C::SXY;
+        const double dn = first ? r[m] : r[m] + beta * D[s];
+        D[s] = dn;
+        if (cl.edge) dpub[par][cl.c0 + m * g.nxy] = dn;
+      }
+      const double *dprev = dpub[par ^ 1];
+      fill_halo<double, TY>(g, a.tiles_x, D, [&](int c) {
+        const double rv = __ldcg(rpub + c);
+        return first ? rv : rv + beta * __ldcg(dprev + c);
+      });
+      __syncthreads();
+      double acc[1] = {0.0};
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) {
+        if (!cl.interior(g, m)) continue;
+        const int s = cl.s0 + m * C::SXY;
+        acc[0] += D[s] * lap_smem<double, C::SX, C::SXY>(g, D, s, cl.i, cl.j, cl.k0 + m);
+      }
+      bsum<1>(acc, scratch);
+      publish<1>(pr.buf(phase), acc);
+      if (!grid_sync(gs)) return;
+      double dq[1];
+      reduce_parts<1>(pr.buf(phase), gridDim.x, dq, scratch);
+      ++phase;
+      if (fabs(dq[0]) < 1e-28) break;  // src/fluid.rs:469
+      const double alpha = delta / dq[0];
+      double acc2[1] = {0.0};
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) {
+        if (!cl.valid(g, m)) continue;
+        const int s = cl.s0 + m * C::SXY;
+        const int c = cl.c0 + m * g.nxy;
+        const double qv =
+            cl.interior(g, m) ? lap_smem<double, C::SX, C::SXY>(g, D, s, cl.i, cl.j, cl.k0 + m)
+                              : 0.0;
+        p[c] = p[c] + alpha * D[s];
+        const double rv = r[m] - alpha * qv;
+        r[m] = rv;
+        if (cl.edge) rpub[c] = rv;
+        acc2[0] += rv * rv;
+      }
+      bsum<1>(acc2, scratch);
+      publish<1>(pr.buf(phase), acc2);
+      if (!grid_sync(gs)) return;
+      double dn[1];
+      reduce_parts<1>(pr.buf(phase), gridDim.x, dn, scratch);
+      ++phase;
+      ++it;
+      last = dn[0];
+      if (!isfinite(dn[0])) break;
+      if (dn[0] < 1e-20) { converged = 1; break; }  // src/fluid.rs:479
+      if (tol2 >= 0.0 && dn[0] <= tol2) { converged = 1; break; }
+      beta = dn[0] / delta;  // src/fluid.rs:482
+      delta = dn[0];
+      par ^= 1;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && a.report) {
+    SolveReport rep;
+    rep.iterations = it;
+    rep.refinements = 0;
+    rep.converged = converged;
+    rep.status = isfinite(last) ? 0 : 4;
+    rep.initial_residual = sqrt(delta0);
+    rep.final_residual = sqrt(last);
+    rep.rhs_norm = sqrt(bb);
+    *a.report = rep;
+  }
+}
+
+// ---------------------------------------------------------------- mixed -----
+// f64 refinement around an f32 CG whose vectors never leave the SM.
+template <int TY, int CPT>
+__global__ void __launch_bounds__(kRT, 1)
+    k_cg_res_mixed(ResidentCgArgs a, GridSync gs, Ring2 pr) {
+  using C = Cells<TY, CPT>;
+  extern __shared__ float Df[];
+  __shared__ double scratch[kRW * 3];
+  const Dims g = a.g;
+  const C cl(g, a.tiles_x);
+  double *p = a.p;
+  const double *b = a.b;
+  float *rpub = static_cast<float *>(a.rpub);
+  float *dpub[2] = {static_cast<float *>(a.dpub0), static_cast<float *>(a.dpub1)};
+  float r[CPT], e[CPT];
+  int phase = 0;
+
+  // r = b - A p in f64, rounded once to f32; e = 0.
+  auto outer_residual = [&](bool with_b) {
+    double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int m = 0; m < CPT; ++m) {
+      r[m] = 0.0f;
+      e[m] = 0.0f;
+      if (!cl.valid(g, m)) continue;
+      const int c = cl.c0 + m * g.nxy;
+      const double ap = cl.interior(g, m) ? lap_global(g, p, c, cl.i, cl.j, cl.k0 + m) : 0.0;
+      const double bc = __ldg(b + c);
+      const double rv = bc - ap;
+      const float rf = float(rv);
+      r[m] = rf;
+      if (cl.edge) rpub[c] = rf;
+      acc[0] += rv * rv;
+      if (with_b) acc[1] += bc * bc;
+      acc[2] += double(rf) * double(rf);
+    }
+    bsum<3>(acc, scratch);
+    publish<3>(pr.buf(phase), acc);
+  };
+
+  outer_residual(true);
+  if (!grid_sync(gs)) return;
+  double tot[3];
+  reduce_parts<3>(pr.buf(phase), gridDim.x, tot, scratch);
+  ++phase;
+  const double bb = tot[1];
+  double rr = tot[0];
+  const double rr0 = rr;
+  double tol2 = -1.0;
+  if (a.rel_tol > 0.0) {
+    const double tl = a.rel_tol * sqrt(bb);
+    tol2 = tl * tl;
+  }
+  int total = 0, passes = 0, converged = 0, par = 0;
+  if (!(rr > 1e-24) || (tol2 >= 0.0 && rr <= tol2)) converged = isfinite(rr) ? 1 : 0;
+
+  while (!converged && passes < a.max_refine && total < a.max_iters && isfinite(rr)) {
+    double inner_rel = a.inner_rel_tol;
+    if (tol2 >= 0.0) inner_rel = fmax(inner_rel, 0.5 * sqrt(tol2 / rr));
+    double delta = tot[2];
+    const double inner_tol2 = inner_rel * inner_rel * delta;
+    double beta = 0.0;
+    int it = 0;
+    while (it < a.max_inner && total < a.max_iters) {
+      const bool first = it == 0;
+      const float bf = float(beta);
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) {
+        if (!cl.valid(g, m)) continue;
+        const int s = cl.s0 + m * C::SXY;
+        const float dn = first ? r[m] : __fmaf_rn(bf, Df[s], r[m]);
+        Df[s] = dn;
+        if (cl.edge) dpub[par][cl.c0 + m * g.nxy] = dn;
+      }
+      const float *dprev = dpub[par ^ 1];
+      fill_halo<float, TY>(g, a.tiles_x, Df, [&](int c) {
+        const float rv = __ldcg(rpub + c);
+        return first ? rv : __fmaf_rn(bf, __ldcg(dprev + c), rv);
+      });
+      __syncthreads();
+      double acc[1] = {0.0};
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) {
+        if (!cl.interior(g, m)) continue;
+        const int s = cl.s0 + m * C::SXY;
+        const float qv = lap_smem<float, C::SX, C::SXY>(g, Df, s, cl.i, cl.j, cl.k0 + m);
+        acc[0] += double(Df[s]) * double(qv);
+      }
+      bsum<1>(acc, scratch);
+      publish<1>(pr.buf(phase), acc);
+      if (!grid_sync(gs)) return;
+      double dq[1];
+      reduce_parts<1>(pr.buf(phase), gridDim.x, dq, scratch);
+      ++phase;
+      if (!(fabs(dq[0]) >= 1e-30)) break;
+      const float af = float(delta / dq[0]);
+      double acc2[1] = {0.0};
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) {
+        if (!cl.valid(g, m)) continue;
+        const int s = cl.s0 + m * C::SXY;
+        const float qv = cl.interior(g, m)
+                             ? lap_smem<float, C::SX, C::SXY>(g, Df, s, cl.i, cl.j, cl.k0 + m)
+                             : 0.0f;
+        e[m] = __fmaf_rn(af, Df[s], e[m]);
+        const float rv = __fmaf_rn(-af, qv, r[m]);
+        r[m] = rv;
+        if (cl.edge) rpub[cl.c0 + m * g.nxy] = rv;
+        acc2[0] += double(rv) * double(rv);
+      }
+      bsum<1>(acc2, scratch);
+      publish<1>(pr.buf(phase), acc2);
+      if (!grid_sync(gs)) return;
+      double dn[1];
+      reduce_parts<1>(pr.buf(phase), gridDim.x, dn, scratch);
+      ++phase;
+      ++it;
+      ++total;
+      par ^= 1;
+      if (!isfinite(dn[0]) || dn[0] <= inner_tol2 || dn[0] < 1e-30) break;
+      beta = dn[0] / delta;
+      delta = dn[0];
+    }
+    // p += e in f64, then the true residual again.
+#pragma unroll
+    for (int m = 0; m < CPT; ++m) {
+      if (!cl.valid(g, m)) continue;
+      const int c = cl.c0 + m * g.nxy;
+      p[c] = p[c] + double(e[m]);
+    }
+    if (!grid_sync(gs)) return;
+    outer_residual(false);
+    if (!grid_sync(gs)) return;
+    reduce_parts<3>(pr.buf(phase), gridDim.x, tot, scratch);
+    ++phase;
+    rr = tot[0];
+    ++passes;
+    if (rr < 1e-20 || (tol2 >= 0.0 && rr <= tol2)) converged = 1;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && a.report) {
+    SolveReport rep;
+    rep.iterations = total;
+    rep.refinements = passes;
+    rep.converged = converged;
+    rep.status = isfinite(rr) ? 0 : 4;
+    rep.initial_residual = sqrt(rr0);
+    rep.final_residual = sqrt(rr);
+    rep.rhs_norm = sqrt(bb);
+    *a.report = rep;
+  }
+}
+
+// ---------------------------------------------------------------- dispatch --
+using KernelFn = void (*)(ResidentCgArgs, GridSync, Ring2);
+
+template <int TY, int CPT>
+KernelFn pick_kernel(bool f64) {
+  return f64 ? &k_cg_res_f64<TY, CPT> : &k_cg_res_mixed<TY, CPT>;
+}
+
+KernelFn kernel_for(bool f64, int ty, int cpt) {
+#define AFL_RES_CASE(TY_, CPT_) \
+  if (ty == TY_ && cpt == CPT_) return pick_kernel<TY_, CPT_>(f64);
+  AFL_RES_CASE(4, 1) AFL_RES_CASE(4, 2) AFL_RES_CASE(4, 4) AFL_RES_CASE(4, 8) AFL_RES_CASE(4, 16)
+  AFL_RES_CASE(8, 1) AFL_RES_CASE(8, 2) AFL_RES_CASE(8, 4) AFL_RES_CASE(8, 8) AFL_RES_CASE(8, 16)
+  AFL_RES_CASE(16, 1) AFL_RES_CASE(16, 2) AFL_RES_CASE(16, 4) AFL_RES_CASE(16, 8)
+  AFL_RES_CASE(16, 16)
+#undef AFL_RES_CASE
+  return nullptr;
+}
+
+}  // namespace
+
+size_t resident_smem_bytes(const Dims &g, int ty, bool f64) {
+  return static_cast<size_t>(kTX + 2) * static_cast<size_t>(ty + 2) *
+         static_cast<size_t>(g.nz) * (f64 ? sizeof(double) : sizeof(float));
+}
+
+bool plan_resident(const Dims &g, bool f64, ResidentPlan *plan) {
+  int dev = 0, sms = 0, smem_optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const size_t static_smem = 2048;  // reduction scratch + barrier flag, rounded up
+  bool found = false;
+  ResidentPlan best{};
+  for (int ty : {4, 8, 16}) {
+    const int groups = kRT / (kTX * ty);
+    int cpt = (g.nz + groups - 1) / groups;
+    int rounded = 1;
+    while (rounded < cpt) rounded *= 2;
+    if (rounded > 16) continue;
+    const int tiles_x = (g.nx + kTX - 1) / kTX;
+    const int tiles_y = (g.ny + ty - 1) / ty;
+    const int tiles = tiles_x * tiles_y;
+    if (tiles > sms) continue;
+    const size_t smem = resident_smem_bytes(g, ty, f64);
+    if (smem + static_smem > static_cast<size_t>(smem_optin)) continue;
+    ResidentPlan cand{ty, rounded, tiles_x, tiles_y, static_cast<int>(smem)};
+    // fewest cells per thread first, then the smaller halo (larger tile)
+    if (!found || cand.cpt < best.cpt || (cand.cpt == best.cpt && cand.ty > best.ty)) {
+      best = cand;
+      found = true;
+    }
+  }
+  if (found && plan) *plan = best;
+  return found;
+}
+
+int launch_cg_resident(const ResidentCgArgs &a, const ResidentPlan &plan, bool f64,
+                       const PersistentState &ps, cudaStream_t st) {
+  KernelFn fn = kernel_for(f64, plan.ty, plan.cpt);
+  if (!fn) return -static_cast<int>(cudaErrorInvalidConfiguration);
+  const int blocks = plan.tiles_x * plan.tiles_y;
+  if (blocks > ps.max_blocks) return -static_cast<int>(cudaErrorInvalidConfiguration);
+  cudaError_t err = cudaFuncSetAttribute(reinterpret_cast<const void *>(fn),
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         plan.smem_bytes);
+  if (err != cudaSuccess) return -static_cast<int>(err);
+  cudaMemsetAsync(ps.count, 0, sizeof(unsigned int), st);
+  cudaMemsetAsync(ps.gen, 0, sizeof(unsigned int), st);
+  cudaMemsetAsync(ps.abort_flag, 0, sizeof(int), st);
+  ResidentCgArgs args = a;
+  args.tiles_x = plan.tiles_x;
+  args.tiles_y = plan.tiles_y;
+  GridSync gs;
+  gs.count = ps.count;
+  gs.gen = ps.gen;
+  gs.abort_flag = ps.abort_flag;
+  gs.nblocks = static_cast<unsigned int>(blocks);
+  gs.timeout_ns = ps.timeout_ns;
+  Ring2 pr{ps.partials, 3 * ps.max_blocks};
+  void *params[] = {&args, &gs, &pr};
+  err = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(fn), dim3(blocks), dim3(kRT),
+                                    params, static_cast<size_t>(plan.smem_bytes), st);
+  return err == cudaSuccess ? blocks : -static_cast<int>(err);
+}
+
+}  // namespace afl

@@ -123,6 +123,8 @@ struct afl_solver {
   int run_cap = 0;
   int *sticky = nullptr;
   afl::PersistentState ps{};
+  bool resident_ok = false;       // the grid fits the on-chip resident CG
+  afl::ResidentPlan resident{};
   double *amp = nullptr;          // sphere amplitude map (optional)
   double *stage = nullptr;        // f64 staging for the mixed form's transfers
   double *sample_buf = nullptr;   // 4 doubles per point
@@ -238,6 +240,8 @@ afl_status validate_params(const afl_params &p) {
     return set_error(AFL_ERR_INVALID_ARGUMENT, "cg_rel_tol must be >= 0");
   if (p.mixed_inner_iters < 1 || p.mixed_max_refinements < 1 || !(p.mixed_inner_rel_tol > 0.0))
     return set_error(AFL_ERR_INVALID_ARGUMENT, "mixed solver settings must be positive");
+  if (p.poisson_kernel < AFL_POISSON_KERNEL_AUTO || p.poisson_kernel > AFL_POISSON_KERNEL_RESIDENT)
+    return set_error(AFL_ERR_INVALID_ARGUMENT, "poisson_kernel must be 0, 1 or 2");
   return AFL_OK;
 }
 
@@ -312,7 +316,29 @@ afl_status stage_solve(afl_solver *s, int kind, int iters, afl::SolveReport *rep
   const Dims &g = s->g;
   StageTimer timer(s, AFL_STAGE_POISSON, 2);
   int blocks = 0;
-  if (s->precision == AFL_PRECISION_FP64) {
+  const bool want_resident = kind == AFL_POISSON_CG &&
+                             s->params.poisson_kernel != AFL_POISSON_KERNEL_STREAMING;
+  if (kind == AFL_POISSON_CG && s->params.poisson_kernel == AFL_POISSON_KERNEL_RESIDENT &&
+      !s->resident_ok)
+    return set_error(AFL_ERR_INVALID_ARGUMENT,
+                     "the %dx%dx%d grid does not fit the resident CG kernel", g.nx, g.ny, g.nz);
+  if (want_resident && s->resident_ok) {
+    const bool f64 = s->precision == AFL_PRECISION_FP64;
+    afl::ResidentCgArgs a{};
+    a.g = g;
+    a.p = s->p;
+    a.b = s->b;
+    a.rpub = s->cg[0];
+    a.dpub0 = f64 ? s->cg[1] : s->cg[2];
+    a.dpub1 = f64 ? s->cg[2] : s->cg[3];
+    a.max_iters = std::max(f64 ? 0 : 1, iters);
+    a.max_inner = std::max(1, s->params.mixed_inner_iters);
+    a.max_refine = s->params.mixed_max_refinements;
+    a.inner_rel_tol = s->params.mixed_inner_rel_tol;
+    a.rel_tol = s->params.cg_rel_tol;
+    a.report = rep;
+    blocks = afl::launch_cg_resident(a, s->resident, f64, s->ps, s->stream);
+  } else if (s->precision == AFL_PRECISION_FP64) {
     if (kind == AFL_POISSON_CG) {
       afl::CgArgs a{g, s->p, s->b, static_cast<double *>(s->cg[0]),
                     static_cast<double *>(s->cg[1]), static_cast<double *>(s->cg[2]),
@@ -526,6 +552,7 @@ afl_status afl_params_default(afl_params *p) {
   p->mixed_inner_iters = 200;
   p->mixed_inner_rel_tol = 1e-4;
   p->mixed_max_refinements = 8;
+  p->poisson_kernel = AFL_POISSON_KERNEL_AUTO;
   return AFL_OK;
 }
 
@@ -589,6 +616,7 @@ afl_status afl_create(size_t nx, size_t ny, size_t nz, const afl_params *params,
                       std::max(afl::persistent_blocks_cg_mixed(),
                                afl::persistent_blocks_sor_mixed()));
   s->ps.max_blocks = maxb;
+  s->resident_ok = afl::plan_resident(s->g, s->precision == AFL_PRECISION_FP64, &s->resident);
   s->ps.timeout_ns = 5000000000ull;  // 5 s per barrier wait
   if (const char *env = std::getenv("AFL_BARRIER_TIMEOUT_NS")) s->ps.timeout_ns = std::strtoull(env, nullptr, 10);
   unsigned int *bar = nullptr;
@@ -1015,6 +1043,16 @@ afl_status afl_get_stage_timing(afl_solver *s, double *ms, int64_t *calls) {
     if (ms) ms[i] = s->stage_ms[i];
     if (calls) calls[i] = s->stage_calls[i];
   }
+  return AFL_OK;
+}
+
+afl_status afl_get_poisson_plan(const afl_solver *s, int32_t out[4]) {
+  AFL_TRY(check_handle(s));
+  if (!out) return set_error(AFL_ERR_INVALID_ARGUMENT, "null output");
+  out[0] = s->resident_ok ? 1 : 0;
+  out[1] = s->resident_ok ? s->resident.ty : 0;
+  out[2] = s->resident_ok ? s->resident.cpt : 0;
+  out[3] = s->resident_ok ? s->resident.tiles_x * s->resident.tiles_y : 0;
   return AFL_OK;
 }
 

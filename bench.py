@@ -181,6 +181,7 @@ def time_form(form: str, n: int, steps: int, warmup: int, dist, torch, rank: int
     stream = torch.cuda.ExternalStream(s.stream)
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
+    plan = s.poisson_plan()
     s.set_stage_timing(True)
     launches0 = s.launch_count()
     if dist:
@@ -199,7 +200,7 @@ def time_form(form: str, n: int, steps: int, warmup: int, dist, torch, rank: int
     fields = {f: s.get_field(f) for f in ("u", "v", "w", "density", "temperature")}
     s.close()
     return {"ms": ms, "infos": infos, "tel": tel, "stages": stages, "launches": launches,
-            "fields": fields, "cells": p.cells}
+            "fields": fields, "cells": p.cells, "plan": plan}
 
 
 def time_e2e(form: str, n: int, steps: int, warmup: int, dist, torch):
@@ -356,6 +357,7 @@ def run_ours(args):
                 "converged_steps": int(sum(i.converged for i in r["infos"])),
                 "step_roofline_frac": sb / (r["ms"] / 1e3) / 1e9 / peak,
                 "stage_ms": {k: round(v[0], 3) for k, v in r["stages"].items()},
+                "poisson_plan": r["plan"] if "cg" in form else None,
             }
         # accuracy of the mixed forms against the f64 GPU forms after K steps
         for mixed, ref in (("mixed_cg", "fp64_cg"), ("mixed_sor", "fp64_sor")):
@@ -389,7 +391,8 @@ def run_ours(args):
             "gpu_launches": int(head["launches"]),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
-                         "kernel": "k_cg_mixed" if headline == "mixed_cg" else headline,
+                         "kernel": ("k_cg_res_mixed" if head["plan"]["resident"] else
+                                    "k_cg_mixed") if headline == "mixed_cg" else headline,
                          "peak_source": peak_kind},
             "variants": variants,
             "adjoint_fwd_ratio": None,

@@ -73,6 +73,15 @@ typedef enum afl_precision {
   AFL_PRECISION_MIXED = 1
 } afl_precision;
 
+/* CG kernel choice.  AUTO: the on-chip resident kernel when the grid fits
+ * (tiles <= SMs, tile + halo in shared memory), else the streaming kernel.
+ * The two differ only in the summation order of the inner products. */
+typedef enum afl_poisson_kernel {
+  AFL_POISSON_KERNEL_AUTO = 0,
+  AFL_POISSON_KERNEL_STREAMING = 1,
+  AFL_POISSON_KERNEL_RESIDENT = 2  /* fails with INVALID_ARGUMENT if it does not fit */
+} afl_poisson_kernel;
+
 /* What step() injects between velocity advection and the forces.
  * CYBERPUNK: inject_cyberpunk_sources (src/fluid.rs:532-595), the reference.
  * SPHERE: assign density/temperature inside a sphere (see afl_params).
@@ -106,9 +115,9 @@ typedef struct afl_params {
   int32_t mixed_inner_iters;  /* MIXED: max f32 CG iterations per refinement
                                  pass (default 200) */
   double mixed_inner_rel_tol; /* MIXED: inner f32 CG relative tolerance
-                                 (default 1e-3) */
+                                 (default 1e-4) */
   int32_t mixed_max_refinements; /* MIXED: max outer passes (default 8) */
-  int32_t reserved_i32;
+  int32_t poisson_kernel; /* afl_poisson_kernel: which CG kernel runs */
   double reserved_f64[4];
 } afl_params;
 
@@ -233,6 +242,11 @@ afl_status afl_set_stage_timing(afl_solver *s, int enable);
  * number of timed calls per stage (arrays of AFL_STAGE_COUNT; either may be
  * NULL). */
 afl_status afl_get_stage_timing(afl_solver *s, double *ms, int64_t *calls);
+/* The CG kernel plan chosen for this grid: out[0] = 1 when the on-chip
+ * resident kernel fits (else the streaming kernel runs), out[1] = tile height
+ * in y (tiles are 16 wide in x and span all z), out[2] = z cells per thread,
+ * out[3] = CTAs (one per SM). */
+afl_status afl_get_poisson_plan(const afl_solver *s, int32_t out[4]);
 /* Kernels this handle has launched since creation. */
 afl_status afl_get_launch_count(const afl_solver *s, uint64_t *count);
 

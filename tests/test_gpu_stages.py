@@ -44,7 +44,8 @@ def pair(af, O, shape, seed=0, vel_scale=1.0, precision=0, **params):
     o = O.OracleSolver(nx, ny, nz)
     if params:
         g.set_params(**params)
-        o.set_params(**{k: v for k, v in params.items() if k != "source_kind"})
+        o.set_params(**{k: v for k, v in params.items()
+                        if k not in ("source_kind", "poisson_kernel")})
     st = seeded_state(shape, seed, vel_scale)
     for f, vals in st.items():
         g.set_field(f, vals)
@@ -120,11 +121,15 @@ def test_rbsor_mixed(af, oracle, shape):
     same(g, o, ["pressure"], precision=1, tol=1e-5)
 
 
+KERNELS = {"streaming": 1, "resident": 2}
+
+
 @pytest.mark.parametrize("shape", SHAPES)
-def test_cg_fixed_iterations(af, oracle, shape):
+@pytest.mark.parametrize("kernel", ["streaming", "resident"])
+def test_cg_fixed_iterations(af, oracle, shape, kernel):
     """Reference stopping rule (absolute), fixed iteration budget: the only
     difference is the summation order of the two inner products."""
-    g, o = pair(af, oracle, shape, seed=19)
+    g, o = pair(af, oracle, shape, seed=19, poisson_kernel=KERNELS[kernel])
     info = g.solve_poisson_conjugate_gradient(30)
     it = o.solve_poisson_conjugate_gradient(30)
     assert info.iterations == it
@@ -133,8 +138,9 @@ def test_cg_fixed_iterations(af, oracle, shape):
 
 
 @pytest.mark.parametrize("shape", [(18, 22, 18), (33, 17, 25)])
-def test_cg_relative_tolerance(af, oracle, shape):
-    g, o = pair(af, oracle, shape, seed=23, cg_rel_tol=1e-6)
+@pytest.mark.parametrize("kernel", ["streaming", "resident"])
+def test_cg_relative_tolerance(af, oracle, shape, kernel):
+    g, o = pair(af, oracle, shape, seed=23, cg_rel_tol=1e-6, poisson_kernel=KERNELS[kernel])
     info = g.solve_poisson_conjugate_gradient(500)
     it = o.solve_poisson_conjugate_gradient(500)
     assert info.converged and abs(info.iterations - it) <= 1
@@ -143,9 +149,11 @@ def test_cg_relative_tolerance(af, oracle, shape):
 
 
 @pytest.mark.parametrize("shape", [(18, 22, 18), (33, 17, 25)])
-def test_cg_mixed_refinement(af, oracle, shape):
+@pytest.mark.parametrize("kernel", ["streaming", "resident"])
+def test_cg_mixed_refinement(af, oracle, shape, kernel):
     """The mixed solve reaches the f64 tolerance in f64 (true residual)."""
-    g, o = pair(af, oracle, shape, seed=29, precision=1, cg_rel_tol=1e-6, solver_iters=2000)
+    g, o = pair(af, oracle, shape, seed=29, precision=1, cg_rel_tol=1e-6, solver_iters=2000,
+                poisson_kernel=KERNELS[kernel])
     info = g.solve_poisson_conjugate_gradient(2000)
     assert info.converged, info
     assert info.final_residual <= 1e-6 * info.rhs_norm
@@ -244,3 +252,25 @@ def test_sample_trilinear(af, oracle, shape):
         c1 = c01 * (1.0 - ty) + c11 * ty
         want.append(c0 * (1.0 - tz) + c1 * tz)
     assert np.array_equal(got, np.array(want))
+
+
+@pytest.mark.parametrize("shape", [(128, 128, 128), (96, 96, 96), (64, 128, 64), (48, 48, 48)])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_resident_matches_streaming_at_full_size(af, shape, precision):
+    """At the workload sizes the resident and streaming kernels solve the same
+    system: 60 fixed iterations agree to summation-order rounding."""
+    nx, ny, nz = shape
+    st = seeded_state(shape, 61, 1.0)
+    out = {}
+    for kernel in ("streaming", "resident"):
+        g = af.FluidSolver3D(nx, ny, nz, precision=precision, poisson_kernel=KERNELS[kernel],
+                             mixed_inner_iters=60, mixed_max_refinements=1)
+        g.set_field("divergence", st["divergence"])
+        g.set_field("pressure", st["pressure"])
+        info = g.solve_poisson_conjugate_gradient(60)
+        assert info.iterations == 60, info
+        out[kernel] = (g.get_field("pressure"), info)
+    tol = 1e-10 if precision == 0 else 1e-4
+    assert rel_l2(out["resident"][0], out["streaming"][0]) <= tol
+    fr, fs = out["resident"][1].final_residual, out["streaming"][1].final_residual
+    assert abs(fr - fs) <= (1e-8 if precision == 0 else 1e-2) * fs
