@@ -25,35 +25,52 @@ constexpr int kRT = 1024;       // threads per CTA
 constexpr int kRW = kRT / 32;   // warps per CTA
 constexpr int kTX = 16;         // tile width in x (cells)
 
+// CTA-wide sum of NV values, valid in every thread.  Warp butterflies, then
+// warp 0 combines the 32 warp sums with another butterfly: a fixed order, so
+// CTAs reducing the same data get the same bits.  `scratch` holds
+// kRW*NV + NV doubles.
 template <int NV>
 __device__ __forceinline__ void bsum(double (&v)[NV], double *scratch) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int a = 0; a < NV; ++a) v[a] = warp_sum(v[a]);
-  __syncthreads();
   if (lane == 0)
 #pragma unroll
     for (int a = 0; a < NV; ++a) scratch[warp * NV + a] = v[a];
   __syncthreads();
+  if (warp == 0) {
 #pragma unroll
-  for (int a = 0; a < NV; ++a) {
-    double s = 0.0;
-    for (int w = 0; w < kRW; ++w) s += scratch[w * NV + a];
-    v[a] = s;
+    for (int a = 0; a < NV; ++a) {
+      const double x = warp_sum(scratch[lane * NV + a]);
+      if (lane == 0) scratch[kRW * NV + a] = x;
+    }
   }
   __syncthreads();
+#pragma unroll
+  for (int a = 0; a < NV; ++a) v[a] = scratch[kRW * NV + a];
 }
 
-// Fixed-order sum of NV interleaved per-CTA partials; identical in every CTA.
+// Fixed-order sum of NV interleaved per-CTA partials, read by warp 0 and
+// broadcast through `slot` (NV doubles); identical in every CTA.
 template <int NV>
 __device__ __forceinline__ void reduce_parts(const double *parts, int nparts,
-                                             double (&out)[NV], double *scratch) {
+                                             double (&out)[NV], double *slot) {
+  if (threadIdx.x < 32) {
+    double acc[NV];
 #pragma unroll
-  for (int a = 0; a < NV; ++a) out[a] = 0.0;
-  for (int b = threadIdx.x; b < nparts; b += kRT)
+    for (int a = 0; a < NV; ++a) acc[a] = 0.0;
+    for (int b = threadIdx.x; b < nparts; b += 32)
 #pragma unroll
-    for (int a = 0; a < NV; ++a) out[a] += __ldcg(parts + b * NV + a);
-  bsum<NV>(out, scratch);
+      for (int a = 0; a < NV; ++a) acc[a] += __ldcg(parts + b * NV + a);
+#pragma unroll
+    for (int a = 0; a < NV; ++a) {
+      acc[a] = warp_sum(acc[a]);
+      if (threadIdx.x == 0) slot[a] = acc[a];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int a = 0; a < NV; ++a) out[a] = slot[a];
 }
 
 template <int NV>
@@ -64,7 +81,8 @@ __device__ __forceinline__ void publish(double *parts, const double (&v)[NV]) {
 }
 
 // Where this thread's cells sit: column (ii, jj) of the tile, planes
-// k0 .. k0+CPT-1.
+// k0 .. k0+CPT-1, and the operator's x/y neighbour tests, which are the same
+// for all of the thread's cells.
 template <int TY, int CPT>
 struct Cells {
   static constexpr int kCols = kTX * TY;
@@ -76,6 +94,7 @@ struct Cells {
   bool in_ij;        // column inside the grid
   bool ij_interior;  // 1 <= i <= nx-2 and 1 <= j <= ny-2
   bool edge;         // value needed by a neighbouring tile
+  bool xl, xh, yl, yh;  // i > 1, i+2 < nx, j > 1, j+2 < ny
   __device__ Cells(const Dims &g, int tiles_x) {
     const int t = threadIdx.x;
     const int col = t % kCols, grp = t / kCols;
@@ -87,6 +106,10 @@ struct Cells {
     in_ij = i < g.nx && j < g.ny;
     ij_interior = i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2;
     edge = ii == 0 || ii == kTX - 1 || jj == 0 || jj == TY - 1;
+    xl = i > 1;
+    xh = i + 2 < g.nx;
+    yl = j > 1;
+    yh = j + 2 < g.ny;
     c0 = (k0 * g.ny + j) * g.nx + i;
     s0 = (k0 * (TY + 2) + jj + 1) * SX + ii + 1;
   }
@@ -97,55 +120,71 @@ struct Cells {
   }
 };
 
-// The reference operator (src/fluid.rs:356-394) on the shared-memory tile.
-template <typename R, int SX, int SXY>
-__device__ __forceinline__ R lap_smem(const Dims &g, const R *D, int s, int i, int j, int k) {
+// The reference operator (src/fluid.rs:356-394) on the shared-memory tile:
+// neighbours summed in the reference's order, missing ones skipped.
+template <typename R, int SX, int SXY, typename Cl>
+__device__ __forceinline__ R lap_smem(const Dims &g, const R *D, int s, const Cl &cl, int k) {
   R diag = R(0), nb = R(0);
-  if (i > 1) { diag += R(1); nb += D[s - 1]; }
-  if (i + 2 < g.nx) { diag += R(1); nb += D[s + 1]; }
-  if (j > 1) { diag += R(1); nb += D[s - SX]; }
-  if (j + 2 < g.ny) { diag += R(1); nb += D[s + SX]; }
+  if (cl.xl) { diag += R(1); nb += D[s - 1]; }
+  if (cl.xh) { diag += R(1); nb += D[s + 1]; }
+  if (cl.yl) { diag += R(1); nb += D[s - SX]; }
+  if (cl.yh) { diag += R(1); nb += D[s + SX]; }
   if (k > 1) { diag += R(1); nb += D[s - SXY]; }
   if (k + 2 < g.nz) { diag += R(1); nb += D[s + SXY]; }
   return diag * D[s] - nb;
 }
 
-// The same operator on the f64 pressure in global memory.
+// The same operator on the f64 pressure in global memory (L2 reads: the
+// pressure is written by other CTAs between passes).
 __device__ __forceinline__ double lap_global(const Dims &g, const double *x, int c, int i, int j,
                                              int k) {
   double diag = 0.0, nb = 0.0;
-  if (i > 1) { diag += 1.0; nb += x[c - 1]; }
-  if (i + 2 < g.nx) { diag += 1.0; nb += x[c + 1]; }
-  if (j > 1) { diag += 1.0; nb += x[c - g.nx]; }
-  if (j + 2 < g.ny) { diag += 1.0; nb += x[c + g.nx]; }
-  if (k > 1) { diag += 1.0; nb += x[c - g.nxy]; }
-  if (k + 2 < g.nz) { diag += 1.0; nb += x[c + g.nxy]; }
-  return diag * x[c] - nb;
+  if (i > 1) { diag += 1.0; nb += __ldcg(x + c - 1); }
+  if (i + 2 < g.nx) { diag += 1.0; nb += __ldcg(x + c + 1); }
+  if (j > 1) { diag += 1.0; nb += __ldcg(x + c - g.nx); }
+  if (j + 2 < g.ny) { diag += 1.0; nb += __ldcg(x + c + g.nx); }
+  if (k > 1) { diag += 1.0; nb += __ldcg(x + c - g.nxy); }
+  if (k + 2 < g.nz) { diag += 1.0; nb += __ldcg(x + c + g.nxy); }
+  return diag * __ldcg(x + c) - nb;
 }
 
-// Rebuilds the halo ring (x and y neighbours of the tile, every plane) from
-// the neighbours' published values: dn = r (first iteration) or dn = f(r, d).
-template <typename R, int TY, typename F>
-__device__ __forceinline__ void fill_halo(const Dims &g, int tiles_x, R *D, const F &value_at) {
-  constexpr int SX = kTX + 2;
-  constexpr int per_plane = 2 * TY + 2 * kTX;
-  const int bx = blockIdx.x % tiles_x, by = blockIdx.x / tiles_x;
-  const int total = per_plane * g.nz;
-  for (int h = threadIdx.x; h < total; h += kRT) {
-    const int k = h / per_plane;
-    const int q = h - k * per_plane;
-    int ii, jj;
+// The halo ring (x and y neighbours of the tile, every plane).  Each thread
+// owns one ring position (ring padded to 64 per plane) in every 16th plane;
+// its column offsets are computed once per solve.
+template <int TY>
+struct Halo {
+  static constexpr int kPerPlane = 2 * TY + 2 * kTX;
+  static constexpr int kPad = 64;
+  static_assert(kPerPlane <= kPad, "ring wider than its padding");
+  static constexpr int kLanes = kRT / kPad;  // planes served per sweep
+  bool active;   // this thread's ring position exists and lies inside the grid
+  int col_c;     // j*nx + i of the ring position
+  int col_s;     // shared offset of the ring position within a plane
+  int k_first;
+  __device__ Halo(const Dims &g, int tiles_x) {
+    constexpr int SX = kTX + 2;
+    const int q = threadIdx.x % kPad;
+    k_first = threadIdx.x / kPad;
+    const int bx = blockIdx.x % tiles_x, by = blockIdx.x / tiles_x;
+    int ii = 0, jj = 0;
     if (q < TY) { ii = -1; jj = q; }
     else if (q < 2 * TY) { ii = kTX; jj = q - TY; }
     else if (q < 2 * TY + kTX) { ii = q - 2 * TY; jj = -1; }
     else { ii = q - 2 * TY - kTX; jj = TY; }
     const int i = bx * kTX + ii, j = by * TY + jj;
-    const int s = (k * (TY + 2) + jj + 1) * SX + ii + 1;
-    R v = R(0);
-    if (i >= 0 && i < g.nx && j >= 0 && j < g.ny) v = value_at((k * g.ny + j) * g.nx + i);
-    D[s] = v;
+    active = q < kPerPlane && i >= 0 && i < g.nx && j >= 0 && j < g.ny;
+    col_c = j * g.nx + i;
+    col_s = (jj + 1) * SX + ii + 1;
   }
-}
+  // D[ring cell] = value_at(global cell) for every plane.
+  template <typename R, typename F>
+  __device__ __forceinline__ void fill(const Dims &g, R *D, const F &value_at) const {
+    constexpr int SXY = (kTX + 2) * (TY + 2);
+    if (!active) return;
+#pragma unroll 4
+    for (int k = k_first; k < g.nz; k += kLanes) D[k * SXY + col_s] = value_at(k * g.nxy + col_c);
+  }
+};
 
 struct Ring2 {
   double *base;
@@ -153,21 +192,27 @@ struct Ring2 {
   __device__ double *buf(int phase) const { return base + (phase & 1) * stride; }
 };
 
+// Shared scratch of the reductions: per-warp values, the CTA result, and the
+// broadcast slot of the grid-wide sums.
+constexpr int kScratch = kRW * 3 + 3 + 3;
+
 // ---------------------------------------------------------------- FP64 ------
 // solve_poisson_conjugate_gradient (src/fluid.rs:445-493) with the relative
-// tolerance extension; p stays in global memory (updated once per iteration).
+// tolerance extension.  d in shared memory, r in registers, p in global memory
+// (updated once per iteration, never read by the operator).
 template <int TY, int CPT>
 __global__ void __launch_bounds__(kRT, 1)
     k_cg_res_f64(ResidentCgArgs a, GridSync gs, Ring2 pr) {
   using C = Cells<TY, CPT>;
   extern __shared__ double D[];
-  __shared__ double scratch[kRW * 2];
+  __shared__ double scratch[kScratch];
+  double *slot = scratch + kRW * 3 + 3;
   const Dims g = a.g;
   const C cl(g, a.tiles_x);
+  const Halo<TY> halo(g, a.tiles_x);
   double *p = a.p;
-  const double *b = a.b;
   double *rpub = static_cast<double *>(a.rpub);
-  double *dpub[2] = {static_cast<double *>(a.dpub0), static_cast<double *>(a.dpub1)};
+  double *dpub0 = static_cast<double *>(a.dpub0), *dpub1 = static_cast<double *>(a.dpub1);
   double r[CPT];
   int phase = 0;
   {
@@ -178,7 +223,7 @@ __global__ void __launch_bounds__(kRT, 1)
       if (!cl.valid(g, m)) continue;
       const int c = cl.c0 + m * g.nxy;
       const double ap = cl.interior(g, m) ? lap_global(g, p, c, cl.i, cl.j, cl.k0 + m) : 0.0;
-      const double bc = __ldg(b + c);
+      const double bc = __ldg(a.b + c);
       const double rv = bc - ap;
       r[m] = rv;
       if (cl.edge) rpub[c] = rv;
@@ -190,7 +235,7 @@ __global__ void __launch_bounds__(kRT, 1)
   }
   if (!grid_sync(gs)) return;
   double tot[2];
-  reduce_parts<2>(pr.buf(phase), gridDim.x, tot, scratch);
+  reduce_parts<2>(pr.buf(phase), gridDim.x, tot, slot);
   ++phase;
   double delta = tot[0];
   const double bb = tot[1];
@@ -208,17 +253,18 @@ __global__ void __launch_bounds__(kRT, 1)
     double beta = 0.0;
     while (it < a.max_iters) {
       const bool first = it == 0;
-      // d = r + beta*d on the tile, published for the neighbours
+      double *dcur = par ? dpub1 : dpub0;
+      const double *dprev = par ? dpub0 : dpub1;
+      // d = r + beta*d on the tile (src/fluid.rs:483-485), edges published
 #pragma unroll
       for (int m = 0; m < CPT; ++m) {
         if (!cl.valid(g, m)) continue;
         const int s = cl.s0 + m * C::SXY;
         const double dn = first ? r[m] : r[m] + beta * D[s];
         D[s] = dn;
-        if (cl.edge) dpub[par][cl.c0 + m * g.nxy] = dn;
+        if (cl.edge) dcur[cl.c0 + m * g.nxy] = dn;
       }
-      const double *dprev = dpub[par ^ 1];
-      fill_halo<double, TY>(g, a.tiles_x, D, [&](int c) {
+      halo.fill(g, D, [&](int c) {
         const double rv = __ldcg(rpub + c);
         return first ? rv : rv + beta * __ldcg(dprev + c);
       });
@@ -228,13 +274,13 @@ __global__ void __launch_bounds__(kRT, 1)
       for (int m = 0; m < CPT; ++m) {
         if (!cl.interior(g, m)) continue;
         const int s = cl.s0 + m * C::SXY;
-        acc[0] += D[s] * lap_smem<double, C::SX, C::SXY>(g, D, s, cl.i, cl.j, cl.k0 + m);
+        acc[0] += D[s] * lap_smem<double, C::SX, C::SXY>(g, D, s, cl, cl.k0 + m);
       }
       bsum<1>(acc, scratch);
       publish<1>(pr.buf(phase), acc);
       if (!grid_sync(gs)) return;
       double dq[1];
-      reduce_parts<1>(pr.buf(phase), gridDim.x, dq, scratch);
+      reduce_parts<1>(pr.buf(phase), gridDim.x, dq, slot);
       ++phase;
       if (fabs(dq[0]) < 1e-28) break;  // src/fluid.rs:469
       const double alpha = delta / dq[0];
@@ -245,8 +291,7 @@ __global__ void __launch_bounds__(kRT, 1)
         const int s = cl.s0 + m * C::SXY;
         const int c = cl.c0 + m * g.nxy;
         const double qv =
-            cl.interior(g, m) ? lap_smem<double, C::SX, C::SXY>(g, D, s, cl.i, cl.j, cl.k0 + m)
-                              : 0.0;
+            cl.interior(g, m) ? lap_smem<double, C::SX, C::SXY>(g, D, s, cl, cl.k0 + m) : 0.0;
         p[c] = p[c] + alpha * D[s];
         const double rv = r[m] - alpha * qv;
         r[m] = rv;
@@ -257,7 +302,7 @@ __global__ void __launch_bounds__(kRT, 1)
       publish<1>(pr.buf(phase), acc2);
       if (!grid_sync(gs)) return;
       double dn[1];
-      reduce_parts<1>(pr.buf(phase), gridDim.x, dn, scratch);
+      reduce_parts<1>(pr.buf(phase), gridDim.x, dn, slot);
       ++phase;
       ++it;
       last = dn[0];
@@ -283,20 +328,23 @@ __global__ void __launch_bounds__(kRT, 1)
 }
 
 // ---------------------------------------------------------------- mixed -----
-// f64 refinement around an f32 CG whose vectors never leave the SM.
+// f64 refinement around an f32 CG whose vectors never leave the SM: d and the
+// correction e in shared memory (same tile layout), r in registers.
 template <int TY, int CPT>
 __global__ void __launch_bounds__(kRT, 1)
     k_cg_res_mixed(ResidentCgArgs a, GridSync gs, Ring2 pr) {
   using C = Cells<TY, CPT>;
   extern __shared__ float Df[];
-  __shared__ double scratch[kRW * 3];
+  __shared__ double scratch[kScratch];
+  double *slot = scratch + kRW * 3 + 3;
   const Dims g = a.g;
   const C cl(g, a.tiles_x);
+  const Halo<TY> halo(g, a.tiles_x);
+  float *E = Df + C::SXY * g.nz;
   double *p = a.p;
-  const double *b = a.b;
   float *rpub = static_cast<float *>(a.rpub);
-  float *dpub[2] = {static_cast<float *>(a.dpub0), static_cast<float *>(a.dpub1)};
-  float r[CPT], e[CPT];
+  float *dpub0 = static_cast<float *>(a.dpub0), *dpub1 = static_cast<float *>(a.dpub1);
+  float r[CPT];
   int phase = 0;
 
   // r = b - A p in f64, rounded once to f32; e = 0.
@@ -305,14 +353,14 @@ __global__ void __launch_bounds__(kRT, 1)
 #pragma unroll
     for (int m = 0; m < CPT; ++m) {
       r[m] = 0.0f;
-      e[m] = 0.0f;
       if (!cl.valid(g, m)) continue;
       const int c = cl.c0 + m * g.nxy;
       const double ap = cl.interior(g, m) ? lap_global(g, p, c, cl.i, cl.j, cl.k0 + m) : 0.0;
-      const double bc = __ldg(b + c);
+      const double bc = __ldg(a.b + c);
       const double rv = bc - ap;
       const float rf = float(rv);
       r[m] = rf;
+      E[cl.s0 + m * C::SXY] = 0.0f;
       if (cl.edge) rpub[c] = rf;
       acc[0] += rv * rv;
       if (with_b) acc[1] += bc * bc;
@@ -325,7 +373,7 @@ __global__ void __launch_bounds__(kRT, 1)
   outer_residual(true);
   if (!grid_sync(gs)) return;
   double tot[3];
-  reduce_parts<3>(pr.buf(phase), gridDim.x, tot, scratch);
+  reduce_parts<3>(pr.buf(phase), gridDim.x, tot, slot);
   ++phase;
   const double bb = tot[1];
   double rr = tot[0];
@@ -348,16 +396,17 @@ __global__ void __launch_bounds__(kRT, 1)
     while (it < a.max_inner && total < a.max_iters) {
       const bool first = it == 0;
       const float bf = float(beta);
+      float *dcur = par ? dpub1 : dpub0;
+      const float *dprev = par ? dpub0 : dpub1;
 #pragma unroll
       for (int m = 0; m < CPT; ++m) {
         if (!cl.valid(g, m)) continue;
         const int s = cl.s0 + m * C::SXY;
         const float dn = first ? r[m] : __fmaf_rn(bf, Df[s], r[m]);
         Df[s] = dn;
-        if (cl.edge) dpub[par][cl.c0 + m * g.nxy] = dn;
+        if (cl.edge) dcur[cl.c0 + m * g.nxy] = dn;
       }
-      const float *dprev = dpub[par ^ 1];
-      fill_halo<float, TY>(g, a.tiles_x, Df, [&](int c) {
+      halo.fill(g, Df, [&](int c) {
         const float rv = __ldcg(rpub + c);
         return first ? rv : __fmaf_rn(bf, __ldcg(dprev + c), rv);
       });
@@ -367,14 +416,14 @@ __global__ void __launch_bounds__(kRT, 1)
       for (int m = 0; m < CPT; ++m) {
         if (!cl.interior(g, m)) continue;
         const int s = cl.s0 + m * C::SXY;
-        const float qv = lap_smem<float, C::SX, C::SXY>(g, Df, s, cl.i, cl.j, cl.k0 + m);
+        const float qv = lap_smem<float, C::SX, C::SXY>(g, Df, s, cl, cl.k0 + m);
         acc[0] += double(Df[s]) * double(qv);
       }
       bsum<1>(acc, scratch);
       publish<1>(pr.buf(phase), acc);
       if (!grid_sync(gs)) return;
       double dq[1];
-      reduce_parts<1>(pr.buf(phase), gridDim.x, dq, scratch);
+      reduce_parts<1>(pr.buf(phase), gridDim.x, dq, slot);
       ++phase;
       if (!(fabs(dq[0]) >= 1e-30)) break;
       const float af = float(delta / dq[0]);
@@ -383,10 +432,9 @@ __global__ void __launch_bounds__(kRT, 1)
       for (int m = 0; m < CPT; ++m) {
         if (!cl.valid(g, m)) continue;
         const int s = cl.s0 + m * C::SXY;
-        const float qv = cl.interior(g, m)
-                             ? lap_smem<float, C::SX, C::SXY>(g, Df, s, cl.i, cl.j, cl.k0 + m)
-                             : 0.0f;
-        e[m] = __fmaf_rn(af, Df[s], e[m]);
+        const float qv =
+            cl.interior(g, m) ? lap_smem<float, C::SX, C::SXY>(g, Df, s, cl, cl.k0 + m) : 0.0f;
+        E[s] = __fmaf_rn(af, Df[s], E[s]);
         const float rv = __fmaf_rn(-af, qv, r[m]);
         r[m] = rv;
         if (cl.edge) rpub[cl.c0 + m * g.nxy] = rv;
@@ -396,7 +444,7 @@ __global__ void __launch_bounds__(kRT, 1)
       publish<1>(pr.buf(phase), acc2);
       if (!grid_sync(gs)) return;
       double dn[1];
-      reduce_parts<1>(pr.buf(phase), gridDim.x, dn, scratch);
+      reduce_parts<1>(pr.buf(phase), gridDim.x, dn, slot);
       ++phase;
       ++it;
       ++total;
@@ -410,12 +458,12 @@ __global__ void __launch_bounds__(kRT, 1)
     for (int m = 0; m < CPT; ++m) {
       if (!cl.valid(g, m)) continue;
       const int c = cl.c0 + m * g.nxy;
-      p[c] = p[c] + double(e[m]);
+      p[c] = p[c] + double(E[cl.s0 + m * C::SXY]);
     }
     if (!grid_sync(gs)) return;
     outer_residual(false);
     if (!grid_sync(gs)) return;
-    reduce_parts<3>(pr.buf(phase), gridDim.x, tot, scratch);
+    reduce_parts<3>(pr.buf(phase), gridDim.x, tot, slot);
     ++phase;
     rr = tot[0];
     ++passes;
@@ -456,8 +504,10 @@ KernelFn kernel_for(bool f64, int ty, int cpt) {
 }  // namespace
 
 size_t resident_smem_bytes(const Dims &g, int ty, bool f64) {
-  return static_cast<size_t>(kTX + 2) * static_cast<size_t>(ty + 2) *
-         static_cast<size_t>(g.nz) * (f64 ? sizeof(double) : sizeof(float));
+  // FP64: the direction tile.  Mixed: direction and correction tiles (f32).
+  const size_t tile = static_cast<size_t>(kTX + 2) * static_cast<size_t>(ty + 2) *
+                      static_cast<size_t>(g.nz);
+  return f64 ? tile * sizeof(double) : 2 * tile * sizeof(float);
 }
 
 bool plan_resident(const Dims &g, bool f64, ResidentPlan *plan) {
