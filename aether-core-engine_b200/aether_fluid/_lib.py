@@ -128,6 +128,8 @@ SIGNATURES = [
     ("afl_get_stage_timing", _st, [_vp, _dp, ctypes.POINTER(ctypes.c_int64)]),
     ("afl_get_poisson_plan", _st, [_vp, ctypes.POINTER(ctypes.c_int32)]),
     ("afl_get_launch_count", _st, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    ("afl_solve_cg_noalloc", _st, [_vp, _vp, _sz, _sz, _sz, _i, _d, _vp,
+                                    ctypes.POINTER(AflSolveInfo)]),
     ("afl_synchronize", _st, [_vp]),
     ("afl_stream", _vp, [_vp]),
 ]

@@ -31,6 +31,7 @@ SOURCES = [
     "afl_poisson_mixed.cu",
     "afl_poisson_resident.cu",
     "afl_solver.cu",
+    "afl_noalloc.cu",
 ]
 
 

@@ -161,6 +161,9 @@ size_t resident_smem_bytes(const Dims &g, int ty, bool f64);
 int launch_cg_resident(const ResidentCgArgs &a, const ResidentPlan &plan, bool f64,
                        const PersistentState &ps, cudaStream_t st);
 
+// Sets the text afl_last_error() returns on the calling thread.
+void set_last_error_text(const char *msg);
+
 // Occupancy-derived CTA count of each persistent kernel (co-residency bound).
 int persistent_blocks_cg_f64();
 int persistent_blocks_sor_f64();

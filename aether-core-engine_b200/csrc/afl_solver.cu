@@ -527,6 +527,10 @@ afl_status check_field(const afl_solver *s, int field, size_t n) {
 
 }  // namespace
 
+namespace afl {
+void set_last_error_text(const char *msg) { g_last_error = msg ? msg : ""; }
+}  // namespace afl
+
 // ============================================================================
 extern "C" {
 

@@ -250,6 +250,26 @@ afl_status afl_get_poisson_plan(const afl_solver *s, int32_t out[4]);
 /* Kernels this handle has launched since creation. */
 afl_status afl_get_launch_count(const afl_solver *s, uint64_t *count);
 
+/* ---- a pressure solve that allocates nothing --------------------------------
+ * No counterpart in the reference.  For callers that may not allocate device
+ * memory -- code recorded into a CUDA graph, real-time/render threads that
+ * must not block on the allocator, hosts whose device memory is one budgeted
+ * pool -- this runs the FP64 CG of afl_solve_cg (same kernel, same stopping
+ * rules, warm start from *d_pressure) on device buffers the caller owns:
+ * d_rhs (read) and d_pressure (read and written), nx*ny*nz doubles each, x
+ * fastest.  Its working memory is a fixed array inside the library (about
+ * 8.1 MiB, held on every GPU that loads the library until exit), so grids
+ * larger than 262144 cells (64^3) are rejected with AFL_ERR_INVALID_ARGUMENT.
+ * The first call on each device looks up that array's device address (with
+ * the device current) and should come before any stream capture.  All calls
+ * share the array: calls whose work overlaps on one GPU race and must be
+ * ordered by the caller.  Runs on `stream` (a cudaStream_t, NULL = legacy
+ * default) and synchronises it before returning; info may be NULL; errors are
+ * reported through afl_last_error(). */
+afl_status afl_solve_cg_noalloc(const double *d_rhs, double *d_pressure, size_t nx, size_t ny,
+                                size_t nz, int max_iters, double rel_tol, void *stream,
+                                afl_solve_info *info);
+
 afl_status afl_synchronize(afl_solver *s);
 /* The handle's cudaStream_t, for callers that order their own work on it. */
 void *afl_stream(afl_solver *s);
