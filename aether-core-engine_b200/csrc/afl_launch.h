@@ -157,7 +157,7 @@ struct ResidentCgArgs {
 // False when the grid does not fit on chip (too many tiles, too much shared
 // memory, or more than 16 z cells per thread).
 bool plan_resident(const Dims &g, bool f64, ResidentPlan *plan);
-size_t resident_smem_bytes(const Dims &g, int ty, bool f64);
+size_t resident_smem_bytes(const Dims &g, int ty, int cpt, bool f64);
 int launch_cg_resident(const ResidentCgArgs &a, const ResidentPlan &plan, bool f64,
                        const PersistentState &ps, cudaStream_t st);
 

@@ -23,7 +23,7 @@ namespace {
 
 constexpr int kRT = 1024;       // threads per CTA
 constexpr int kRW = kRT / 32;   // warps per CTA
-constexpr int kTX = 16;         // tile width in x (cells)
+constexpr int kTX = 16;         // tile width in x (cells): one half-warp reads one row
 
 // CTA-wide sum of NV values, valid in every thread.  Warp butterflies, then
 // warp 0 combines the 32 warp sums with another butterfly: a fixed order, so
@@ -73,32 +73,63 @@ __device__ __forceinline__ void reduce_parts(const double *parts, int nparts,
   for (int a = 0; a < NV; ++a) out[a] = slot[a];
 }
 
+// Sums NV values over the CTA (same fixed order as bsum) and stores the CTA's
+// partials to parts[blockIdx.x*NV + a]; only warp 0 sees the sum, so one CTA
+// barrier suffices (the grid barrier that follows starts with another).
 template <int NV>
-__device__ __forceinline__ void publish(double *parts, const double (&v)[NV]) {
-  if (threadIdx.x == 0)
+__device__ __forceinline__ void publish_sum(double *parts, double (&v)[NV], double *scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int a = 0; a < NV; ++a) parts[blockIdx.x * NV + a] = v[a];
+  for (int a = 0; a < NV; ++a) v[a] = warp_sum(v[a]);
+  if (lane == 0)
+#pragma unroll
+    for (int a = 0; a < NV; ++a) scratch[warp * NV + a] = v[a];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int a = 0; a < NV; ++a) {
+      const double x = warp_sum(scratch[lane * NV + a]);
+      if (lane == 0) parts[blockIdx.x * NV + a] = x;
+    }
+  }
 }
 
 // Where this thread's cells sit: column (ii, jj) of the tile, planes
 // k0 .. k0+CPT-1, and the operator's x/y neighbour tests, which are the same
 // for all of the thread's cells.
+// Shared-memory plane stride: the (kTX+2) x (TY+2) plane padded to an odd
+// number of words, so that the two half-warps (which work CPT planes apart)
+// hit disjoint banks.
+template <int TY>
+struct Plane {
+  static constexpr int SX = kTX + 2;
+  static constexpr int kRaw = (kTX + 2) * (TY + 2);
+  static constexpr int SXY = kRaw | 1;
+};
+
 template <int TY, int CPT>
 struct Cells {
   static constexpr int kCols = kTX * TY;
-  static_assert(kRT % kCols == 0, "a CTA must cover whole column groups");
-  static constexpr int SX = kTX + 2;
-  static constexpr int SXY = (kTX + 2) * (TY + 2);
+  static_assert(kRT % (2 * kCols) == 0, "a CTA must cover whole pairs of column groups");
+  static constexpr int SX = Plane<TY>::SX;
+  static constexpr int SXY = Plane<TY>::SXY;
+  static constexpr int kPlanes = (kRT / kCols) * CPT;  // planes the threads cover (>= nz)
   int i, j, k0;
   int c0, s0;        // global / shared index of plane k0
   bool in_ij;        // column inside the grid
   bool ij_interior;  // 1 <= i <= nx-2 and 1 <= j <= ny-2
   bool edge;         // value needed by a neighbouring tile
   bool xl, xh, yl, yh;  // i > 1, i+2 < nx, j > 1, j+2 < ny
+  int diag_xy;          // x/y neighbours present (the operator's diagonal part)
   __device__ Cells(const Dims &g, int tiles_x) {
+    // lane bits 0-3: x in the tile; bit 4: which of a pair of plane groups;
+    // then the row jj, then the group pair.
     const int t = threadIdx.x;
-    const int col = t % kCols, grp = t / kCols;
-    const int ii = col % kTX, jj = col / kTX;
+    const int ii = t & (kTX - 1);
+    const int half = (t >> 4) & 1;
+    const int row_pair = t >> 5;
+    const int jj = row_pair % TY;
+    const int grp = 2 * (row_pair / TY) + half;
     const int bx = blockIdx.x % tiles_x, by = blockIdx.x / tiles_x;
     i = bx * kTX + ii;
     j = by * TY + jj;
@@ -110,8 +141,9 @@ struct Cells {
     xh = i + 2 < g.nx;
     yl = j > 1;
     yh = j + 2 < g.ny;
+    diag_xy = int(xl) + int(xh) + int(yl) + int(yh);
     c0 = (k0 * g.ny + j) * g.nx + i;
-    s0 = (k0 * (TY + 2) + jj + 1) * SX + ii + 1;
+    s0 = k0 * SXY + (jj + 1) * SX + ii + 1;
   }
   __device__ bool valid(const Dims &g, int m) const { return in_ij && k0 + m < g.nz; }
   __device__ bool interior(const Dims &g, int m) const {
@@ -120,17 +152,21 @@ struct Cells {
   }
 };
 
-// The reference operator (src/fluid.rs:356-394) on the shared-memory tile:
-// neighbours summed in the reference's order, missing ones skipped.
+// The reference operator (src/fluid.rs:356-394) on the shared-memory tile,
+// without branches: a missing neighbour contributes a selected 0 to the sum
+// (the reference skips it; the sum is the same value), the diagonal is the
+// count of present neighbours.  Shared slots of missing neighbours are never
+// used, whatever they hold.
 template <typename R, int SX, int SXY, typename Cl>
 __device__ __forceinline__ R lap_smem(const Dims &g, const R *D, int s, const Cl &cl, int k) {
-  R diag = R(0), nb = R(0);
-  if (cl.xl) { diag += R(1); nb += D[s - 1]; }
-  if (cl.xh) { diag += R(1); nb += D[s + 1]; }
-  if (cl.yl) { diag += R(1); nb += D[s - SX]; }
-  if (cl.yh) { diag += R(1); nb += D[s + SX]; }
-  if (k > 1) { diag += R(1); nb += D[s - SXY]; }
-  if (k + 2 < g.nz) { diag += R(1); nb += D[s + SXY]; }
+  const bool zl = k > 1, zh = k + 2 < g.nz;
+  R nb = cl.xl ? D[s - 1] : R(0);
+  nb += cl.xh ? D[s + 1] : R(0);
+  nb += cl.yl ? D[s - SX] : R(0);
+  nb += cl.yh ? D[s + SX] : R(0);
+  nb += zl ? D[s - SXY] : R(0);
+  nb += zh ? D[s + SXY] : R(0);
+  const R diag = R(cl.diag_xy + int(zl) + int(zh));
   return diag * D[s] - nb;
 }
 
@@ -148,41 +184,49 @@ __device__ __forceinline__ double lap_global(const Dims &g, const double *x, int
   return diag * __ldcg(x + c) - nb;
 }
 
-// The halo ring (x and y neighbours of the tile, every plane).  Each thread
-// owns one ring position (ring padded to 64 per plane) in every 16th plane;
-// its column offsets are computed once per solve.
+// The halo ring (x and y neighbours of the tile, every plane): 2*TY + 2*kTX
+// cells per plane, padded to kPad so that each thread keeps one ring position
+// (computed once) and serves it in every kLanes-th plane.  Ring positions
+// outside the grid are skipped (the operator never reads them).  The ring
+// keeps last iteration's directions, so a new ring direction needs only the
+// neighbour's published residual: d = r + beta*d_ring, the owner's expression
+// on the owner's operands.
 template <int TY>
 struct Halo {
   static constexpr int kPerPlane = 2 * TY + 2 * kTX;
-  static constexpr int kPad = 64;
-  static_assert(kPerPlane <= kPad, "ring wider than its padding");
-  static constexpr int kLanes = kRT / kPad;  // planes served per sweep
-  bool active;   // this thread's ring position exists and lies inside the grid
-  int col_c;     // j*nx + i of the ring position
-  int col_s;     // shared offset of the ring position within a plane
-  int k_first;
+  static constexpr int kPad = kPerPlane <= 64 ? 64 : 128;
+  static constexpr int kLanes = kRT / kPad;
+  bool active;
+  int col_c, col_s, k_first;
   __device__ Halo(const Dims &g, int tiles_x) {
-    constexpr int SX = kTX + 2;
+    constexpr int SX = Plane<TY>::SX;
     const int q = threadIdx.x % kPad;
     k_first = threadIdx.x / kPad;
-    const int bx = blockIdx.x % tiles_x, by = blockIdx.x / tiles_x;
-    int ii = 0, jj = 0;
-    if (q < TY) { ii = -1; jj = q; }
-    else if (q < 2 * TY) { ii = kTX; jj = q - TY; }
-    else if (q < 2 * TY + kTX) { ii = q - 2 * TY; jj = -1; }
-    else { ii = q - 2 * TY - kTX; jj = TY; }
-    const int i = bx * kTX + ii, j = by * TY + jj;
+    const int bx0 = (blockIdx.x % tiles_x) * kTX, by0 = (blockIdx.x / tiles_x) * TY;
+    int ii, jj;
+    if (q < 2 * kTX) {  // the rows below and above the tile
+      jj = q < kTX ? -1 : TY;
+      ii = q < kTX ? q : q - kTX;
+    } else {            // the columns left and right of the tile
+      const int r = q - 2 * kTX;
+      ii = r < TY ? -1 : kTX;
+      jj = r < TY ? r : r - TY;
+    }
+    const int i = bx0 + ii, j = by0 + jj;
     active = q < kPerPlane && i >= 0 && i < g.nx && j >= 0 && j < g.ny;
     col_c = j * g.nx + i;
     col_s = (jj + 1) * SX + ii + 1;
   }
-  // D[ring cell] = value_at(global cell) for every plane.
+  // D[ring cell] = value_at(global cell, D[ring cell]) for every plane.
   template <typename R, typename F>
   __device__ __forceinline__ void fill(const Dims &g, R *D, const F &value_at) const {
-    constexpr int SXY = (kTX + 2) * (TY + 2);
+    constexpr int SXY = Plane<TY>::SXY;
     if (!active) return;
 #pragma unroll 4
-    for (int k = k_first; k < g.nz; k += kLanes) D[k * SXY + col_s] = value_at(k * g.nxy + col_c);
+    for (int k = k_first; k < g.nz; k += kLanes) {
+      R &slot = D[k * SXY + col_s];
+      slot = value_at(k * g.nxy + col_c, slot);
+    }
   }
 };
 
@@ -204,7 +248,8 @@ template <int TY, int CPT>
 __global__ void __launch_bounds__(kRT, 1)
     k_cg_res_f64(ResidentCgArgs a, GridSync gs, Ring2 pr) {
   using C = Cells<TY, CPT>;
-  extern __shared__ double D[];
+  extern __shared__ double Dbase[];
+  double *D = Dbase + C::SXY;  // one padding plane below plane 0
   __shared__ double scratch[kScratch];
   double *slot = scratch + kRW * 3 + 3;
   const Dims g = a.g;
@@ -212,7 +257,6 @@ __global__ void __launch_bounds__(kRT, 1)
   const Halo<TY> halo(g, a.tiles_x);
   double *p = a.p;
   double *rpub = static_cast<double *>(a.rpub);
-  double *dpub0 = static_cast<double *>(a.dpub0), *dpub1 = static_cast<double *>(a.dpub1);
   double r[CPT];
   int phase = 0;
   {
@@ -230,8 +274,7 @@ __global__ void __launch_bounds__(kRT, 1)
       acc[0] += rv * rv;
       acc[1] += bc * bc;
     }
-    bsum<2>(acc, scratch);
-    publish<2>(pr.buf(phase), acc);
+    publish_sum<2>(pr.buf(phase), acc, scratch);
   }
   if (!grid_sync(gs)) return;
   double tot[2];
@@ -246,38 +289,34 @@ __global__ void __launch_bounds__(kRT, 1)
   }
   const double delta0 = delta;
   double last = delta;
-  int it = 0, converged = 0, par = 0;
+  int it = 0, converged = 0;
   if (!(delta > 1e-24) || (tol2 >= 0.0 && delta <= tol2)) {
     converged = isfinite(delta) ? 1 : 0;
   } else {
     double beta = 0.0;
     while (it < a.max_iters) {
       const bool first = it == 0;
-      double *dcur = par ? dpub1 : dpub0;
-      const double *dprev = par ? dpub0 : dpub1;
-      // d = r + beta*d on the tile (src/fluid.rs:483-485), edges published
+      // d = r + beta*d on the tile and its halo ring (src/fluid.rs:483-485).
+      // Cells past the grid hold r = 0, so their d stays 0: the loops below
+      // need no per-cell branches (padding planes keep every slot in bounds).
 #pragma unroll
       for (int m = 0; m < CPT; ++m) {
-        if (!cl.valid(g, m)) continue;
         const int s = cl.s0 + m * C::SXY;
-        const double dn = first ? r[m] : r[m] + beta * D[s];
-        D[s] = dn;
-        if (cl.edge) dcur[cl.c0 + m * g.nxy] = dn;
+        D[s] = first ? r[m] : r[m] + beta * D[s];
       }
-      halo.fill(g, D, [&](int c) {
+      halo.fill(g, D, [&](int c, double dprev) {
         const double rv = __ldcg(rpub + c);
-        return first ? rv : rv + beta * __ldcg(dprev + c);
+        return first ? rv : rv + beta * dprev;
       });
       __syncthreads();
       double acc[1] = {0.0};
 #pragma unroll
       for (int m = 0; m < CPT; ++m) {
-        if (!cl.interior(g, m)) continue;
         const int s = cl.s0 + m * C::SXY;
-        acc[0] += D[s] * lap_smem<double, C::SX, C::SXY>(g, D, s, cl, cl.k0 + m);
+        const double qv = lap_smem<double, C::SX, C::SXY>(g, D, s, cl, cl.k0 + m);
+        acc[0] += cl.interior(g, m) ? D[s] * qv : 0.0;
       }
-      bsum<1>(acc, scratch);
-      publish<1>(pr.buf(phase), acc);
+      publish_sum<1>(pr.buf(phase), acc, scratch);
       if (!grid_sync(gs)) return;
       double dq[1];
       reduce_parts<1>(pr.buf(phase), gridDim.x, dq, slot);
@@ -287,19 +326,18 @@ __global__ void __launch_bounds__(kRT, 1)
       double acc2[1] = {0.0};
 #pragma unroll
       for (int m = 0; m < CPT; ++m) {
-        if (!cl.valid(g, m)) continue;
         const int s = cl.s0 + m * C::SXY;
         const int c = cl.c0 + m * g.nxy;
-        const double qv =
-            cl.interior(g, m) ? lap_smem<double, C::SX, C::SXY>(g, D, s, cl, cl.k0 + m) : 0.0;
-        p[c] = p[c] + alpha * D[s];
+        const double lq = lap_smem<double, C::SX, C::SXY>(g, D, s, cl, cl.k0 + m);
+        const double qv = cl.interior(g, m) ? lq : 0.0;
+        const bool v = cl.valid(g, m);
+        if (v) p[c] = p[c] + alpha * D[s];
         const double rv = r[m] - alpha * qv;
         r[m] = rv;
-        if (cl.edge) rpub[c] = rv;
+        if (v && cl.edge) rpub[c] = rv;
         acc2[0] += rv * rv;
       }
-      bsum<1>(acc2, scratch);
-      publish<1>(pr.buf(phase), acc2);
+      publish_sum<1>(pr.buf(phase), acc2, scratch);
       if (!grid_sync(gs)) return;
       double dn[1];
       reduce_parts<1>(pr.buf(phase), gridDim.x, dn, slot);
@@ -311,7 +349,6 @@ __global__ void __launch_bounds__(kRT, 1)
       if (tol2 >= 0.0 && dn[0] <= tol2) { converged = 1; break; }
       beta = dn[0] / delta;  // src/fluid.rs:482
       delta = dn[0];
-      par ^= 1;
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && a.report) {
@@ -334,16 +371,16 @@ template <int TY, int CPT>
 __global__ void __launch_bounds__(kRT, 1)
     k_cg_res_mixed(ResidentCgArgs a, GridSync gs, Ring2 pr) {
   using C = Cells<TY, CPT>;
-  extern __shared__ float Df[];
+  extern __shared__ float Dfbase[];
+  float *Df = Dfbase + C::SXY;  // one padding plane below plane 0
   __shared__ double scratch[kScratch];
   double *slot = scratch + kRW * 3 + 3;
   const Dims g = a.g;
   const C cl(g, a.tiles_x);
   const Halo<TY> halo(g, a.tiles_x);
-  float *E = Df + C::SXY * g.nz;
+  float *E = Df + C::SXY * (C::kPlanes + 2);  // the correction, same tile layout
   double *p = a.p;
   float *rpub = static_cast<float *>(a.rpub);
-  float *dpub0 = static_cast<float *>(a.dpub0), *dpub1 = static_cast<float *>(a.dpub1);
   float r[CPT];
   int phase = 0;
 
@@ -353,6 +390,7 @@ __global__ void __launch_bounds__(kRT, 1)
 #pragma unroll
     for (int m = 0; m < CPT; ++m) {
       r[m] = 0.0f;
+      E[cl.s0 + m * C::SXY] = 0.0f;
       if (!cl.valid(g, m)) continue;
       const int c = cl.c0 + m * g.nxy;
       const double ap = cl.interior(g, m) ? lap_global(g, p, c, cl.i, cl.j, cl.k0 + m) : 0.0;
@@ -360,14 +398,12 @@ __global__ void __launch_bounds__(kRT, 1)
       const double rv = bc - ap;
       const float rf = float(rv);
       r[m] = rf;
-      E[cl.s0 + m * C::SXY] = 0.0f;
       if (cl.edge) rpub[c] = rf;
       acc[0] += rv * rv;
       if (with_b) acc[1] += bc * bc;
       acc[2] += double(rf) * double(rf);
     }
-    bsum<3>(acc, scratch);
-    publish<3>(pr.buf(phase), acc);
+    publish_sum<3>(pr.buf(phase), acc, scratch);
   };
 
   outer_residual(true);
@@ -383,7 +419,7 @@ __global__ void __launch_bounds__(kRT, 1)
     const double tl = a.rel_tol * sqrt(bb);
     tol2 = tl * tl;
   }
-  int total = 0, passes = 0, converged = 0, par = 0;
+  int total = 0, passes = 0, converged = 0;
   if (!(rr > 1e-24) || (tol2 >= 0.0 && rr <= tol2)) converged = isfinite(rr) ? 1 : 0;
 
   while (!converged && passes < a.max_refine && total < a.max_iters && isfinite(rr)) {
@@ -396,31 +432,24 @@ __global__ void __launch_bounds__(kRT, 1)
     while (it < a.max_inner && total < a.max_iters) {
       const bool first = it == 0;
       const float bf = float(beta);
-      float *dcur = par ? dpub1 : dpub0;
-      const float *dprev = par ? dpub0 : dpub1;
 #pragma unroll
       for (int m = 0; m < CPT; ++m) {
-        if (!cl.valid(g, m)) continue;
         const int s = cl.s0 + m * C::SXY;
-        const float dn = first ? r[m] : __fmaf_rn(bf, Df[s], r[m]);
-        Df[s] = dn;
-        if (cl.edge) dcur[cl.c0 + m * g.nxy] = dn;
+        Df[s] = first ? r[m] : __fmaf_rn(bf, Df[s], r[m]);
       }
-      halo.fill(g, Df, [&](int c) {
+      halo.fill(g, Df, [&](int c, float dprev) {
         const float rv = __ldcg(rpub + c);
-        return first ? rv : __fmaf_rn(bf, __ldcg(dprev + c), rv);
+        return first ? rv : __fmaf_rn(bf, dprev, rv);
       });
       __syncthreads();
       double acc[1] = {0.0};
 #pragma unroll
       for (int m = 0; m < CPT; ++m) {
-        if (!cl.interior(g, m)) continue;
         const int s = cl.s0 + m * C::SXY;
         const float qv = lap_smem<float, C::SX, C::SXY>(g, Df, s, cl, cl.k0 + m);
-        acc[0] += double(Df[s]) * double(qv);
+        acc[0] += cl.interior(g, m) ? double(Df[s]) * double(qv) : 0.0;
       }
-      bsum<1>(acc, scratch);
-      publish<1>(pr.buf(phase), acc);
+      publish_sum<1>(pr.buf(phase), acc, scratch);
       if (!grid_sync(gs)) return;
       double dq[1];
       reduce_parts<1>(pr.buf(phase), gridDim.x, dq, slot);
@@ -430,25 +459,22 @@ __global__ void __launch_bounds__(kRT, 1)
       double acc2[1] = {0.0};
 #pragma unroll
       for (int m = 0; m < CPT; ++m) {
-        if (!cl.valid(g, m)) continue;
         const int s = cl.s0 + m * C::SXY;
-        const float qv =
-            cl.interior(g, m) ? lap_smem<float, C::SX, C::SXY>(g, Df, s, cl, cl.k0 + m) : 0.0f;
+        const float lq = lap_smem<float, C::SX, C::SXY>(g, Df, s, cl, cl.k0 + m);
+        const float qv = cl.interior(g, m) ? lq : 0.0f;
         E[s] = __fmaf_rn(af, Df[s], E[s]);
         const float rv = __fmaf_rn(-af, qv, r[m]);
         r[m] = rv;
-        if (cl.edge) rpub[cl.c0 + m * g.nxy] = rv;
+        if (cl.edge && cl.valid(g, m)) rpub[cl.c0 + m * g.nxy] = rv;
         acc2[0] += double(rv) * double(rv);
       }
-      bsum<1>(acc2, scratch);
-      publish<1>(pr.buf(phase), acc2);
+      publish_sum<1>(pr.buf(phase), acc2, scratch);
       if (!grid_sync(gs)) return;
       double dn[1];
       reduce_parts<1>(pr.buf(phase), gridDim.x, dn, slot);
       ++phase;
       ++it;
       ++total;
-      par ^= 1;
       if (!isfinite(dn[0]) || dn[0] <= inner_tol2 || dn[0] < 1e-30) break;
       beta = dn[0] / delta;
       delta = dn[0];
@@ -503,10 +529,14 @@ KernelFn kernel_for(bool f64, int ty, int cpt) {
 
 }  // namespace
 
-size_t resident_smem_bytes(const Dims &g, int ty, bool f64) {
+size_t resident_smem_bytes(const Dims &g, int ty, int cpt, bool f64) {
   // FP64: the direction tile.  Mixed: direction and correction tiles (f32).
-  const size_t tile = static_cast<size_t>(kTX + 2) * static_cast<size_t>(ty + 2) *
-                      static_cast<size_t>(g.nz);
+  // Planes: those the threads cover (groups*cpt >= nz) plus one padding plane
+  // on each side, so every shared access of the branch-free loops is in bounds.
+  (void)g;
+  const size_t plane = static_cast<size_t>((kTX + 2) * (ty + 2)) | 1u;
+  const size_t planes = static_cast<size_t>(kRT / (kTX * ty)) * cpt + 2;
+  const size_t tile = plane * planes;
   return f64 ? tile * sizeof(double) : 2 * tile * sizeof(float);
 }
 
@@ -528,7 +558,7 @@ bool plan_resident(const Dims &g, bool f64, ResidentPlan *plan) {
     const int tiles_y = (g.ny + ty - 1) / ty;
     const int tiles = tiles_x * tiles_y;
     if (tiles > sms) continue;
-    const size_t smem = resident_smem_bytes(g, ty, f64);
+    const size_t smem = resident_smem_bytes(g, ty, rounded, f64);
     if (smem + static_smem > static_cast<size_t>(smem_optin)) continue;
     ResidentPlan cand{ty, rounded, tiles_x, tiles_y, static_cast<int>(smem)};
     // fewest cells per thread first, then the smaller halo (larger tile)
