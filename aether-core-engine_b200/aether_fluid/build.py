@@ -23,13 +23,15 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
           "--expt-relaxed-constexpr", "-extended-lambda"]
 # Units whose f64 arithmetic must not be contracted into FMAs.
-NO_FMA = {"afl_kernels_f64.cu", "afl_poisson_f64.cu", "afl_poisson_resident.cu"}
+NO_FMA = {"afl_kernels_f64.cu", "afl_poisson_f64.cu", "afl_poisson_resident.cu",
+          "afl_poisson_stream.cu"}
 SOURCES = [
     "afl_kernels_f64.cu",
     "afl_kernels_f32.cu",
     "afl_poisson_f64.cu",
     "afl_poisson_mixed.cu",
     "afl_poisson_resident.cu",
+    "afl_poisson_stream.cu",
     "afl_solver.cu",
     "afl_noalloc.cu",
 ]

@@ -164,6 +164,13 @@ int launch_cg_resident(const ResidentCgArgs &a, const ResidentPlan &plan, bool f
 // Sets the text afl_last_error() returns on the calling thread.
 void set_last_error_text(const char *msg);
 
+// Streaming CG (afl_poisson_stream.cu): x runs of 2 doubles / 4 floats per
+// thread when nx allows, else single cells.
+int stream_vector_width(const Dims &g, bool f64);
+int launch_cg_stream_f64(const CgArgs &a, const PersistentState &ps, cudaStream_t st);
+int launch_cg_stream_mixed(const MixedCgArgs &a, const PersistentState &ps, cudaStream_t st);
+int persistent_blocks_stream();
+
 // Occupancy-derived CTA count of each persistent kernel (co-residency bound).
 int persistent_blocks_cg_f64();
 int persistent_blocks_sor_f64();

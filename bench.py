@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=128, help="grid edge (default 128)")
+    ap.add_argument("--seed", type=int, default=0, help="velocity-noise seed (default 0)")
     ap.add_argument("--forms", default="mixed_cg,fp64_cg,fp64_sor,mixed_sor")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -64,11 +65,14 @@ def parse():
     return ap.parse_args()
 
 
+SEED = 0
+
+
 def plume_for(form: str, n: int):
     from aether_fluid.plume import Plume
     if form.endswith("sor"):
-        return Plume(n, n, n, 200, seed=0, solver="sor", iters=80)
-    return Plume(n, n, n, 200, seed=0)
+        return Plume(n, n, n, 200, seed=SEED, solver="sor", iters=80)
+    return Plume(n, n, n, 200, seed=SEED)
 
 
 # ---------------------------------------------------------------- clocks -----
@@ -459,7 +463,9 @@ def run_reference(args):
 
 
 def main():
+    global SEED
     args = parse()
+    SEED = args.seed
     if args.impl == "reference":
         run_reference(args)
     else:
