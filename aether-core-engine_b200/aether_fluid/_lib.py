@@ -80,6 +80,19 @@ class AflSolveInfo(ctypes.Structure):
     ]
 
 
+class AflInstance(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_size_t), ("ny", ctypes.c_size_t), ("nz", ctypes.c_size_t),
+        ("seed", ctypes.c_uint64),
+        ("noise_lo", ctypes.c_double), ("noise_hi", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("vorticity_eps", ctypes.c_double), ("buoyancy_beta", ctypes.c_double),
+        ("gravity_alpha", ctypes.c_double),
+        ("sphere_center", ctypes.c_double * 3), ("sphere_radius", ctypes.c_double),
+        ("sphere_density", ctypes.c_double), ("sphere_temperature", ctypes.c_double),
+    ]
+
+
 class AetherFluidError(RuntimeError):
     def __init__(self, status: int, message: str):
         self.status = status
@@ -128,6 +141,16 @@ SIGNATURES = [
     ("afl_get_stage_timing", _st, [_vp, _dp, ctypes.POINTER(ctypes.c_int64)]),
     ("afl_get_poisson_plan", _st, [_vp, ctypes.POINTER(ctypes.c_int32)]),
     ("afl_get_launch_count", _st, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    ("afl_ensemble_create", _st, [ctypes.POINTER(AflInstance), _i, ctypes.POINTER(AflParams),
+                                   ctypes.POINTER(_vp)]),
+    ("afl_ensemble_destroy", _st, [_vp]),
+    ("afl_ensemble_run", _st, [_vp, _i, ctypes.POINTER(AflTelemetry),
+                               ctypes.POINTER(AflSolveInfo)]),
+    ("afl_ensemble_download_field", _st, [_vp, _i, _i, _dp, _sz]),
+    ("afl_ensemble_autotune", _st, [_vp, ctypes.POINTER(ctypes.c_int32)]),
+    ("afl_ensemble_info", _st, [_vp, ctypes.POINTER(ctypes.c_int32)]),
+    ("afl_ensemble_instance_ctas", _st, [_vp, ctypes.POINTER(ctypes.c_int32), _i]),
+    ("afl_rng_f64", _st, [ctypes.c_uint64, ctypes.c_uint64, _sz, _dp]),
     ("afl_solve_cg_noalloc", _st, [_vp, _vp, _sz, _sz, _sz, _i, _d, _vp,
                                     ctypes.POINTER(AflSolveInfo)]),
     ("afl_synchronize", _st, [_vp]),

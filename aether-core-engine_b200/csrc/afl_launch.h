@@ -171,6 +171,60 @@ int launch_cg_stream_f64(const CgArgs &a, const PersistentState &ps, cudaStream_
 int launch_cg_stream_mixed(const MixedCgArgs &a, const PersistentState &ps, cudaStream_t st);
 int persistent_blocks_stream();
 
+// One system of the batched (multi-grid) streaming CG: its arguments, its own
+// barrier and partials (2 buffers x 3 values x ctas), and its CTA range.
+struct MultiCgSystem {
+  CgArgs f64;          // used by the FP64 form
+  MixedCgArgs mixed;   // used by the mixed form
+  GridSync gs;         // nblocks = ctas
+  double *partials;
+  int cta_begin, ctas;
+};
+// d_sys / d_cta_inst live in device memory; every system's grid must allow the
+// vector width v (nx % v == 0).
+int launch_cg_multi(const MultiCgSystem *d_sys, const int *d_cta_inst, int total_ctas, bool f64,
+                    int v, cudaStream_t st);
+int persistent_blocks_multi(bool f64, int v);
+
+// ---- ensemble (afl_ensemble_kernels.cuh) ------------------------------------
+// Device-side descriptor of one instance of a batched ensemble.
+template <typename T>
+struct EnsInstance {
+  Dims g;
+  T *fld[5];        // current u, v, w, density, temperature
+  T *tmp_fwd, *tmp_out;
+  T *curl[4];
+  double *p, *b;
+  T scale_f, scale_b, dt, eps_h, inv_2h, beta, alpha;
+  double h, inv_h, dv, inv_2h_d, dt_time;
+  int src_on;                 // sphere source active
+  int src_lo[3], src_hi[3];   // clamped bounding box (src/fluid.rs:566-571 rule)
+  double src_c[3], src_r2, src_rho, src_temp;
+  int blk_begin, blk_count;   // plane blocks of this instance in the block table
+};
+
+template <typename T>
+struct EnsLaunch {
+  EnsInstance<T> *inst;  // device descriptors
+  const int *blk_inst;   // device block table: plane block -> instance
+  int blocks;            // plane blocks of all instances
+  int count;             // instances
+};
+
+template <typename T>
+void ens_advect(const EnsLaunch<T> &L, int f, double diss, cudaStream_t st);
+template <typename T>
+void ens_forces(const EnsLaunch<T> &L, cudaStream_t st);
+template <typename T>
+void ens_divergence(const EnsLaunch<T> &L, cudaStream_t st);
+template <typename T>
+void ens_project(const EnsLaunch<T> &L, cudaStream_t st);
+template <typename T>
+void ens_telemetry(const EnsLaunch<T> &L, double *partials, const int *step_counter,
+                   double *tel_out, const SolveReport *rep_cur, SolveReport *reports,
+                   int capacity, cudaStream_t st);
+void ens_step_advance(int *step_counter, cudaStream_t st);
+
 // Occupancy-derived CTA count of each persistent kernel (co-residency bound).
 int persistent_blocks_cg_f64();
 int persistent_blocks_sor_f64();

@@ -159,7 +159,8 @@ __device__ __forceinline__ void lap_p_run(const Dims &g, const Run &ru, const do
 }
 
 template <int NV>
-__device__ __forceinline__ void cta_publish(double *parts, double (&v)[NV], double *scratch) {
+__device__ __forceinline__ void cta_publish(double *parts, int vblock, double (&v)[NV],
+                                            double *scratch) {
   constexpr int W = kST / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -172,7 +173,7 @@ __device__ __forceinline__ void cta_publish(double *parts, double (&v)[NV], doub
 #pragma unroll
     for (int a = 0; a < NV; ++a) {
       const double x = warp_sum(lane < W ? scratch[lane * NV + a] : 0.0);
-      if (lane == 0) parts[blockIdx.x * NV + a] = x;
+      if (lane == 0) parts[vblock * NV + a] = x;
     }
   }
 }
@@ -205,13 +206,16 @@ struct Ring3 {
 };
 
 // ------------------------------------------------------------------ FP64 ----
+// The solve run by CTA `vblock` of `vgrid` CTAs working on this system (the
+// whole launch for a single grid, a slice of it in the batched launch).
 template <int V>
-__global__ void __launch_bounds__(kST) k_cg_stream_f64(CgArgs a, GridSync gs, Ring3 pr) {
-  __shared__ double scratch[(kST / 32) * 2 + 4];
+__device__ __forceinline__ void cg_stream_f64_body(const CgArgs &a, const GridSync &gs,
+                                                   const Ring3 &pr, int vblock, int vgrid,
+                                                   double *scratch) {
   double *slot = scratch + (kST / 32) * 2;
   const Dims g = a.g;
   const int runs = g.n / V;
-  const int t0 = blockIdx.x * kST + threadIdx.x, stride = gridDim.x * kST;
+  const int t0 = vblock * kST + threadIdx.x, stride = vgrid * kST;
   double *p = a.p, *r = a.r, *q = a.q;
   const double *b = a.b;
   int phase = 0;
@@ -231,11 +235,11 @@ __global__ void __launch_bounds__(kST) k_cg_stream_f64(CgArgs a, GridSync gs, Ri
       }
       stv<double, V>(r + ru.c, rv);
     }
-    cta_publish<2>(pr.buf(phase), acc, scratch);
+    cta_publish<2>(pr.buf(phase), vblock, acc, scratch);
   }
   if (!grid_sync(gs)) return;
   double tot[2];
-  grid_total<2>(pr.buf(phase), gridDim.x, tot, slot);
+  grid_total<2>(pr.buf(phase), vgrid, tot, slot);
   ++phase;
   double delta = tot[0];
   const double bb = tot[1];
@@ -264,10 +268,10 @@ __global__ void __launch_bounds__(kST) k_cg_stream_f64(CgArgs a, GridSync gs, Ri
 #pragma unroll
         for (int e = 0; e < V; ++e) acc[0] += dn.v[e] * qv.v[e];
       }
-      cta_publish<1>(pr.buf(phase), acc, scratch);
+      cta_publish<1>(pr.buf(phase), vblock, acc, scratch);
       if (!grid_sync(gs)) return;
       double dq[1];
-      grid_total<1>(pr.buf(phase), gridDim.x, dq, slot);
+      grid_total<1>(pr.buf(phase), vgrid, dq, slot);
       ++phase;
       if (fabs(dq[0]) < 1e-28) break;  // src/fluid.rs:469
       const double alpha = delta / dq[0];
@@ -287,10 +291,10 @@ __global__ void __launch_bounds__(kST) k_cg_stream_f64(CgArgs a, GridSync gs, Ri
         stv<double, V>(p + c, pv);
         stv<double, V>(r + c, rv);
       }
-      cta_publish<1>(pr.buf(phase), acc2, scratch);
+      cta_publish<1>(pr.buf(phase), vblock, acc2, scratch);
       if (!grid_sync(gs)) return;
       double dn[1];
-      grid_total<1>(pr.buf(phase), gridDim.x, dn, slot);
+      grid_total<1>(pr.buf(phase), vgrid, dn, slot);
       ++phase;
       ++it;
       last = dn[0];
@@ -304,7 +308,7 @@ __global__ void __launch_bounds__(kST) k_cg_stream_f64(CgArgs a, GridSync gs, Ri
       dnew = t;
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0 && a.report) {
+  if (vblock == 0 && threadIdx.x == 0 && a.report) {
     SolveReport rep;
     rep.iterations = it;
     rep.refinements = 0;
@@ -319,12 +323,13 @@ __global__ void __launch_bounds__(kST) k_cg_stream_f64(CgArgs a, GridSync gs, Ri
 
 // ----------------------------------------------------------------- mixed ----
 template <int V>
-__global__ void __launch_bounds__(kST) k_cg_stream_mixed(MixedCgArgs a, GridSync gs, Ring3 pr) {
-  __shared__ double scratch[(kST / 32) * 3 + 4];
+__device__ __forceinline__ void cg_stream_mixed_body(const MixedCgArgs &a, const GridSync &gs,
+                                                     const Ring3 &pr, int vblock, int vgrid,
+                                                     double *scratch) {
   double *slot = scratch + (kST / 32) * 3;
   const Dims g = a.g;
   const int runs = g.n / V;
-  const int t0 = blockIdx.x * kST + threadIdx.x, stride = gridDim.x * kST;
+  const int t0 = vblock * kST + threadIdx.x, stride = vgrid * kST;
   double *p = a.p;
   const double *b = a.b;
   float *r = a.r, *e = a.e, *q = a.q;
@@ -350,13 +355,13 @@ __global__ void __launch_bounds__(kST) k_cg_stream_mixed(MixedCgArgs a, GridSync
       stv<float, V>(r + ru.c, rf);
       stv<float, V>(e + ru.c, zero);
     }
-    cta_publish<3>(pr.buf(phase), acc, scratch);
+    cta_publish<3>(pr.buf(phase), vblock, acc, scratch);
   };
 
   outer_residual(true);
   if (!grid_sync(gs)) return;
   double tot[3];
-  grid_total<3>(pr.buf(phase), gridDim.x, tot, slot);
+  grid_total<3>(pr.buf(phase), vgrid, tot, slot);
   ++phase;
   const double bb = tot[1];
   double rr = tot[0];
@@ -390,10 +395,10 @@ __global__ void __launch_bounds__(kST) k_cg_stream_mixed(MixedCgArgs a, GridSync
 #pragma unroll
         for (int x = 0; x < V; ++x) acc[0] += double(dn.v[x]) * double(qv.v[x]);
       }
-      cta_publish<1>(pr.buf(phase), acc, scratch);
+      cta_publish<1>(pr.buf(phase), vblock, acc, scratch);
       if (!grid_sync(gs)) return;
       double dq[1];
-      grid_total<1>(pr.buf(phase), gridDim.x, dq, slot);
+      grid_total<1>(pr.buf(phase), vgrid, dq, slot);
       ++phase;
       if (!(fabs(dq[0]) >= 1e-30)) break;
       const float af = float(delta / dq[0]);
@@ -413,10 +418,10 @@ __global__ void __launch_bounds__(kST) k_cg_stream_mixed(MixedCgArgs a, GridSync
         stv<float, V>(e + c, ev);
         stv<float, V>(r + c, rv);
       }
-      cta_publish<1>(pr.buf(phase), acc2, scratch);
+      cta_publish<1>(pr.buf(phase), vblock, acc2, scratch);
       if (!grid_sync(gs)) return;
       double dn[1];
-      grid_total<1>(pr.buf(phase), gridDim.x, dn, slot);
+      grid_total<1>(pr.buf(phase), vgrid, dn, slot);
       ++phase;
       ++it;
       ++total;
@@ -439,13 +444,13 @@ __global__ void __launch_bounds__(kST) k_cg_stream_mixed(MixedCgArgs a, GridSync
     if (!grid_sync(gs)) return;
     outer_residual(false);
     if (!grid_sync(gs)) return;
-    grid_total<3>(pr.buf(phase), gridDim.x, tot, slot);
+    grid_total<3>(pr.buf(phase), vgrid, tot, slot);
     ++phase;
     rr = tot[0];
     ++passes;
     if (rr < 1e-20 || (tol2 >= 0.0 && rr <= tol2)) converged = 1;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0 && a.report) {
+  if (vblock == 0 && threadIdx.x == 0 && a.report) {
     SolveReport rep;
     rep.iterations = total;
     rep.refinements = passes;
@@ -455,6 +460,38 @@ __global__ void __launch_bounds__(kST) k_cg_stream_mixed(MixedCgArgs a, GridSync
     rep.final_residual = sqrt(rr);
     rep.rhs_norm = sqrt(bb);
     *a.report = rep;
+  }
+}
+
+template <int V>
+__global__ void __launch_bounds__(kST) k_cg_stream_f64(CgArgs a, GridSync gs, Ring3 pr) {
+  __shared__ double scratch[(kST / 32) * 3 + 4];
+  cg_stream_f64_body<V>(a, gs, pr, blockIdx.x, gridDim.x, scratch);
+}
+
+template <int V>
+__global__ void __launch_bounds__(kST) k_cg_stream_mixed(MixedCgArgs a, GridSync gs, Ring3 pr) {
+  __shared__ double scratch[(kST / 32) * 3 + 4];
+  cg_stream_mixed_body<V>(a, gs, pr, blockIdx.x, gridDim.x, scratch);
+}
+
+// Many independent solves in one cooperative launch: CTA b works on system
+// cta_inst[b] as its (b - first CTA of that system)-th CTA; each system has its
+// own barrier, partials and stopping decisions, so systems finish at their
+// own iteration counts.
+template <int V, bool F64>
+__global__ void __launch_bounds__(kST) k_cg_stream_multi(const MultiCgSystem *sys,
+                                                         const int *cta_inst) {
+  __shared__ double scratch[(kST / 32) * 3 + 4];
+  const MultiCgSystem &s = sys[cta_inst[blockIdx.x]];
+  const int vblock = blockIdx.x - s.cta_begin;
+  const Ring3 pr{s.partials, (F64 ? 2 : 3) * s.ctas};
+  if constexpr (F64) {
+    const CgArgs a = s.f64;
+    cg_stream_f64_body<V>(a, s.gs, pr, vblock, s.ctas, scratch);
+  } else {
+    const MixedCgArgs a = s.mixed;
+    cg_stream_mixed_body<V>(a, s.gs, pr, vblock, s.ctas, scratch);
   }
 }
 
@@ -492,6 +529,27 @@ int launch_persistent(K kernel, const Args &a, const PersistentState &ps, int nv
 }
 
 }  // namespace
+
+int persistent_blocks_multi(bool f64, int v) {
+  if (f64) return v == 2 ? blocks_of(&k_cg_stream_multi<2, true>)
+                         : blocks_of(&k_cg_stream_multi<1, true>);
+  return v == 4 ? blocks_of(&k_cg_stream_multi<4, false>) : blocks_of(&k_cg_stream_multi<1, false>);
+}
+
+int launch_cg_multi(const MultiCgSystem *d_sys, const int *d_cta_inst, int total_ctas, bool f64,
+                    int v, cudaStream_t st) {
+  const void *fn;
+  if (f64)
+    fn = v == 2 ? reinterpret_cast<const void *>(&k_cg_stream_multi<2, true>)
+                : reinterpret_cast<const void *>(&k_cg_stream_multi<1, true>);
+  else
+    fn = v == 4 ? reinterpret_cast<const void *>(&k_cg_stream_multi<4, false>)
+                : reinterpret_cast<const void *>(&k_cg_stream_multi<1, false>);
+  void *params[] = {const_cast<MultiCgSystem **>(&d_sys), const_cast<int **>(&d_cta_inst)};
+  const cudaError_t err =
+      cudaLaunchCooperativeKernel(fn, dim3(total_ctas), dim3(kST), params, 0, st);
+  return err == cudaSuccess ? total_ctas : -static_cast<int>(err);
+}
 
 int persistent_blocks_stream() {
   const int a = blocks_of(&k_cg_stream_f64<1>), b = blocks_of(&k_cg_stream_f64<2>);

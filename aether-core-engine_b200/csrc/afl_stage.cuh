@@ -28,15 +28,18 @@ __device__ __forceinline__ bool cell_of_thread(const Dims &g, int &i, int &j, in
   return i < g.nx && j < g.ny;
 }
 
+// Each stage is a per-cell device function (shared by the single-grid kernels
+// below and the batched ensemble kernels of afl_ensemble.cu, so both run the
+// same arithmetic) plus a thin kernel over one grid.
+
 // ---- MacCormack advection (src/fluid.rs:153-234) ---------------------------
 // Pass 1: fwd = SL(src, dt) -- advect_semi_lagrangian (src/fluid.rs:153-167).
 template <typename T>
-__global__ void __launch_bounds__(kTx *kTy)
-    k_advect_fwd(Dims g, const T *__restrict__ u, const T *__restrict__ v,
-                 const T *__restrict__ w, const T *__restrict__ src, T *__restrict__ fwd,
-                 T scale) {
-  int i, j, k;
-  if (!cell_of_thread(g, i, j, k)) return;
+__device__ __forceinline__ void cell_advect_fwd(const Dims &g, const T *__restrict__ u,
+                                                const T *__restrict__ v,
+                                                const T *__restrict__ w,
+                                                const T *__restrict__ src, T *__restrict__ fwd,
+                                                T scale, int i, int j, int k) {
   const int c = (k * g.ny + j) * g.nx + i;
   T out = T(0);
   if (interior(g, i, j, k)) {
@@ -48,18 +51,28 @@ __global__ void __launch_bounds__(kTx *kTy)
   fwd[c] = out;
 }
 
+template <typename T>
+__global__ void __launch_bounds__(kTx *kTy)
+    k_advect_fwd(Dims g, const T *__restrict__ u, const T *__restrict__ v,
+                 const T *__restrict__ w, const T *__restrict__ src, T *__restrict__ fwd,
+                 T scale) {
+  int i, j, k;
+  if (!cell_of_thread(g, i, j, k)) return;
+  cell_advect_fwd(g, u, v, w, src, fwd, scale, i, j, k);
+}
+
 // Pass 2: the reference's bwd = SL(fwd, -dt) (:184) is evaluated on the fly at
 // each cell, then the MacCormack correction with the 8-cell clamp, the
 // near-wall fallback, dissipation and max(0) for scalars (:186-229).  The
 // result goes to a separate buffer: src is read at data-dependent cells.
 template <typename T>
-__global__ void __launch_bounds__(kTx *kTy)
-    k_advect_mc(Dims g, const T *__restrict__ u, const T *__restrict__ v,
-                const T *__restrict__ w, const T *__restrict__ src,
-                const T *__restrict__ fwd, T *__restrict__ out, T scale_f, T scale_b,
-                T dissipation, int nonneg) {
-  int i, j, k;
-  if (!cell_of_thread(g, i, j, k)) return;
+__device__ __forceinline__ void cell_advect_mc(const Dims &g, const T *__restrict__ u,
+                                               const T *__restrict__ v,
+                                               const T *__restrict__ w,
+                                               const T *__restrict__ src,
+                                               const T *__restrict__ fwd, T *__restrict__ out,
+                                               T scale_f, T scale_b, T dissipation, int nonneg,
+                                               int i, int j, int k) {
   const int c = (k * g.ny + j) * g.nx + i;
   T res = T(0);
   if (interior(g, i, j, k)) {
@@ -90,6 +103,17 @@ __global__ void __launch_bounds__(kTx *kTy)
   out[c] = res;
 }
 
+template <typename T>
+__global__ void __launch_bounds__(kTx *kTy)
+    k_advect_mc(Dims g, const T *__restrict__ u, const T *__restrict__ v,
+                const T *__restrict__ w, const T *__restrict__ src,
+                const T *__restrict__ fwd, T *__restrict__ out, T scale_f, T scale_b,
+                T dissipation, int nonneg) {
+  int i, j, k;
+  if (!cell_of_thread(g, i, j, k)) return;
+  cell_advect_mc(g, u, v, w, src, fwd, out, scale_f, scale_b, dissipation, nonneg, i, j, k);
+}
+
 // ---- enforce_wall_velocity_bc (src/fluid.rs:236-253) -----------------------
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
@@ -105,12 +129,11 @@ __global__ void __launch_bounds__(kTx *kTy)
 // ---- vorticity confinement + buoyancy (src/fluid.rs:256-330) ---------------
 // Pass 1: central-difference curl and |omega| on the interior (:260-281).
 template <typename T>
-__global__ void __launch_bounds__(kTx *kTy)
-    k_curl(Dims g, const T *__restrict__ u, const T *__restrict__ v,
-           const T *__restrict__ w, T *__restrict__ cx, T *__restrict__ cy,
-           T *__restrict__ cz, T *__restrict__ cmag, T inv_2h) {
-  int i, j, k;
-  if (!cell_of_thread(g, i, j, k)) return;
+__device__ __forceinline__ void cell_curl(const Dims &g, const T *__restrict__ u,
+                                          const T *__restrict__ v, const T *__restrict__ w,
+                                          T *__restrict__ cx, T *__restrict__ cy,
+                                          T *__restrict__ cz, T *__restrict__ cmag, T inv_2h,
+                                          int i, int j, int k) {
   const int c = (k * g.ny + j) * g.nx + i;
   if (!interior(g, i, j, k)) {
     cx[c] = T(0);
@@ -135,17 +158,28 @@ __global__ void __launch_bounds__(kTx *kTy)
   cmag[c] = sqrt(ox * ox + oy * oy + oz * oz);
 }
 
-// Pass 2: confinement force on 2..n-3 (:284-316), buoyancy lift on 1..n-2
-// (:318-327) and the wall BC (:329), fused; pointwise in u/v/w, so in place.
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
-    k_confine_buoy(Dims g, T *__restrict__ u, T *__restrict__ v, T *__restrict__ w,
-                   const T *__restrict__ rho, const T *__restrict__ temp,
-                   const T *__restrict__ cx, const T *__restrict__ cy,
-                   const T *__restrict__ cz, const T *__restrict__ cmag, T dt, T eps_h,
-                   T inv_2h, T beta, T alpha) {
+    k_curl(Dims g, const T *__restrict__ u, const T *__restrict__ v,
+           const T *__restrict__ w, T *__restrict__ cx, T *__restrict__ cy,
+           T *__restrict__ cz, T *__restrict__ cmag, T inv_2h) {
   int i, j, k;
   if (!cell_of_thread(g, i, j, k)) return;
+  cell_curl(g, u, v, w, cx, cy, cz, cmag, inv_2h, i, j, k);
+}
+
+// Pass 2: confinement force on 2..n-3 (:284-316), buoyancy lift on 1..n-2
+// (:318-327) and the wall BC (:329), fused; pointwise in u/v/w, so in place.
+// `rho_c`/`temp_c` are the density and temperature at the cell.
+template <typename T>
+__device__ __forceinline__ void cell_confine_buoy(const Dims &g, T *__restrict__ u,
+                                                  T *__restrict__ v, T *__restrict__ w,
+                                                  T rho_c, T temp_c, const T *__restrict__ cx,
+                                                  const T *__restrict__ cy,
+                                                  const T *__restrict__ cz,
+                                                  const T *__restrict__ cmag, T dt, T eps_h,
+                                                  T inv_2h, T beta, T alpha, int i, int j,
+                                                  int k) {
   const int c = (k * g.ny + j) * g.nx + i;
   T uu = u[c], vv = v[c], ww = w[c];
   if (i >= 2 && i <= g.nx - 3 && j >= 2 && j <= g.ny - 3 && k >= 2 && k <= g.nz - 3) {
@@ -164,12 +198,26 @@ __global__ void __launch_bounds__(kTx *kTy)
     ww = ww + dt * fz;
   }
   if (interior(g, i, j, k)) {
-    const T lift = beta * temp[c] - alpha * rho[c];
+    const T lift = beta * temp_c - alpha * rho_c;
     vv = vv + dt * lift;
   }
   u[c] = wall_u(g, i, j, k) ? T(0) : uu;
   v[c] = wall_v(g, i, j, k) ? T(0) : vv;
   w[c] = wall_w(g, i, j, k) ? T(0) : ww;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTx *kTy)
+    k_confine_buoy(Dims g, T *__restrict__ u, T *__restrict__ v, T *__restrict__ w,
+                   const T *__restrict__ rho, const T *__restrict__ temp,
+                   const T *__restrict__ cx, const T *__restrict__ cy,
+                   const T *__restrict__ cz, const T *__restrict__ cmag, T dt, T eps_h,
+                   T inv_2h, T beta, T alpha) {
+  int i, j, k;
+  if (!cell_of_thread(g, i, j, k)) return;
+  const int c = (k * g.ny + j) * g.nx + i;
+  cell_confine_buoy(g, u, v, w, rho[c], temp[c], cx, cy, cz, cmag, dt, eps_h, inv_2h, beta,
+                    alpha, i, j, k);
 }
 
 // ---- compute_divergence_norm (src/fluid.rs:333-353) ------------------------
@@ -215,11 +263,10 @@ __global__ void __launch_bounds__(kBlock)
 // gradient is formed in f64; in the mixed form the f32 velocity is updated in
 // f64 and rounded once.
 template <typename T>
-__global__ void __launch_bounds__(kTx *kTy)
-    k_project(Dims g, T *__restrict__ u, T *__restrict__ v, T *__restrict__ w,
-              const double *__restrict__ p, double inv_h) {
-  int i, j, k;
-  if (!cell_of_thread(g, i, j, k)) return;
+__device__ __forceinline__ void cell_project(const Dims &g, T *__restrict__ u,
+                                             T *__restrict__ v, T *__restrict__ w,
+                                             const double *__restrict__ p, double inv_h, int i,
+                                             int j, int k) {
   const int c = (k * g.ny + j) * g.nx + i;
   if (interior(g, i, j, k)) {
     const double pc = p[c];
@@ -230,6 +277,15 @@ __global__ void __launch_bounds__(kTx *kTy)
   if (wall_u(g, i, j, k)) u[c] = T(0);
   if (wall_v(g, i, j, k)) v[c] = T(0);
   if (wall_w(g, i, j, k)) w[c] = T(0);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTx *kTy)
+    k_project(Dims g, T *__restrict__ u, T *__restrict__ v, T *__restrict__ w,
+              const double *__restrict__ p, double inv_h) {
+  int i, j, k;
+  if (!cell_of_thread(g, i, j, k)) return;
+  cell_project(g, u, v, w, p, inv_h, i, j, k);
 }
 
 // ---- sources -----------------------------------------------------------------

@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=128, help="grid edge (default 128)")
     ap.add_argument("--seed", type=int, default=0, help="velocity-noise seed (default 0)")
+    ap.add_argument("--poisson-kernel", type=int, default=0,
+                    help="CG kernel: 0 auto, 1 streaming, 2 on-chip resident")
     ap.add_argument("--forms", default="mixed_cg,fp64_cg,fp64_sor,mixed_sor")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -66,6 +68,7 @@ def parse():
 
 
 SEED = 0
+POISSON_KERNEL = 0
 
 
 def plume_for(form: str, n: int):
@@ -179,6 +182,7 @@ def time_form(form: str, n: int, steps: int, warmup: int, dist, torch, rank: int
     import aether_fluid as af
     p = plume_for(form, n)
     s = p.build(precision=af.Precision.MIXED if form.startswith("mixed") else af.Precision.FP64)
+    s.set_params(poisson_kernel=POISSON_KERNEL)
     if warmup > 0:
         s.run(warmup, p.dt, 0.0, p.dt)
     s.init_velocity_noise(p.seed)  # back to the initial state, outside the timed region
@@ -463,9 +467,10 @@ def run_reference(args):
 
 
 def main():
-    global SEED
+    global SEED, POISSON_KERNEL
     args = parse()
     SEED = args.seed
+    POISSON_KERNEL = args.poisson_kernel
     if args.impl == "reference":
         run_reference(args)
     else:

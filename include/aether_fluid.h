@@ -250,6 +250,48 @@ afl_status afl_get_poisson_plan(const afl_solver *s, int32_t out[4]);
 /* Kernels this handle has launched since creation. */
 afl_status afl_get_launch_count(const afl_solver *s, uint64_t *count);
 
+/* ---- batched ensemble (no reference counterpart) -----------------------------
+ * Many independent plumes of different grid sizes advanced together: every
+ * stage of a step is one batched launch over all instances, the pressure
+ * solves run in one cooperative launch whose CTAs are split between the
+ * instances, and one step is captured once in a CUDA graph and replayed.
+ * Each instance follows step() with the sphere source (the same arithmetic
+ * as a single solver with the same settings; only reduction order differs). */
+typedef struct afl_instance {
+  size_t nx, ny, nz;
+  uint64_t seed;           /* velocity noise: Rng::from_seed(seed), range_f64 */
+  double noise_lo, noise_hi;
+  double dt;               /* time step of this instance */
+  double vorticity_eps, buoyancy_beta, gravity_alpha;
+  double sphere_center[3]; /* cell-index coordinates */
+  double sphere_radius;    /* cells; 0 = no source */
+  double sphere_density, sphere_temperature;
+} afl_instance;
+
+typedef struct afl_ensemble afl_ensemble;
+
+/* common: precision, solver_iters, cg_rel_tol and the mixed_* knobs apply to
+ * every instance (CG only); NULL for the defaults. */
+afl_status afl_ensemble_create(const afl_instance *instances, int count,
+                               const afl_params *common, afl_ensemble **out);
+afl_status afl_ensemble_destroy(afl_ensemble *e);
+/* `steps` steps of every instance; telemetry and infos (either may be NULL)
+ * receive steps*count entries, step-major.  Telemetry time is n*dt. */
+afl_status afl_ensemble_run(afl_ensemble *e, int steps, afl_telemetry *telemetry,
+                            afl_solve_info *infos);
+afl_status afl_ensemble_download_field(afl_ensemble *e, int instance, int field, double *host,
+                                       size_t n);
+/* Picks the CTA split of the batched solve by timing candidates on a snapshot
+ * of the state (restored afterwards); *choice gets the candidate index. */
+afl_status afl_ensemble_autotune(afl_ensemble *e, int32_t *choice);
+/* out = {instances, step graph captured (1/0), solver CTAs, co-resident CTA
+ * budget, vector width, autotune choice (-1 = not tuned)} */
+afl_status afl_ensemble_info(const afl_ensemble *e, int32_t out[6]);
+afl_status afl_ensemble_instance_ctas(const afl_ensemble *e, int32_t *out, int count);
+/* The reference generator (src/rng.rs:21-88): n values of next_f64 after
+ * skipping `skip` next_u64 draws from Rng::from_seed(seed). */
+afl_status afl_rng_f64(uint64_t seed, uint64_t skip, size_t n, double *out);
+
 /* ---- a pressure solve that allocates nothing --------------------------------
  * No counterpart in the reference.  For callers that may not allocate device
  * memory -- code recorded into a CUDA graph, real-time/render threads that
