@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--forms", default="mixed_cg,fp64_cg,fp64_sor,mixed_sor")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="skip the 48-plume batched-ensemble measurement")
+    ap.add_argument("--ensemble-steps", type=int, default=100)
     ap.add_argument("--cpu-seconds", type=float, default=20.0,
                     help="target length of the bounded CPU sample")
     return ap.parse_args()
@@ -259,6 +262,48 @@ def time_e2e(form: str, n: int, steps: int, warmup: int, dist, torch):
     return {"seconds": el, "h2d_per_step": h2d / steps, "d2h_per_step": d2h / steps}
 
 
+def time_ensemble(steps: int, torch):
+    """The 48-plume ensemble (mixed CG to 1e-6): one batched, graph-captured
+    run of `steps` steps against the same 48 plumes run one at a time through
+    single-grid solvers.  Device time; states start from the initial
+    condition."""
+    import aether_fluid as af
+    from aether_fluid.ensemble import Ensemble, plume48
+    specs = plume48()
+    cells = sum(s.cells for s in specs)
+    ens = Ensemble(specs, precision=af.Precision.MIXED)
+    choice = ens.autotune()
+    info = ens.info()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, infos = ens.run(steps)
+    torch.cuda.synchronize()
+    batched = time.perf_counter() - t0
+    its = [i.iterations for row in infos for i in row]
+    ens.close()
+    single_s = 0.0
+    for sp in specs:
+        s = af.FluidSolver3D(sp.nx, sp.ny, sp.nz, precision=af.Precision.MIXED)
+        s.set_params(vorticity_eps=sp.eps, buoyancy_beta=sp.beta, gravity_alpha=sp.alpha,
+                     solver_kind=0, solver_iters=200, cg_rel_tol=1e-6)
+        s.init_velocity_noise(sp.seed, -sp.noise, sp.noise)
+        s.set_sphere_source(sp.center, sp.radius)
+        s.run(1, sp.dt)                 # warm the kernels (untimed)
+        s.init_velocity_noise(sp.seed, -sp.noise, sp.noise)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.run(steps, sp.dt, 0.0, sp.dt)
+        torch.cuda.synchronize()
+        single_s += time.perf_counter() - t0
+        s.close()
+    return {"instances": len(specs), "cells": cells, "steps": steps,
+            "batched_mcell_steps_per_s": cells * steps / batched / 1e6,
+            "one_at_a_time_mcell_steps_per_s": cells * steps / single_s / 1e6,
+            "speedup": single_s / batched, "batched_s": batched, "one_at_a_time_s": single_s,
+            "graph": info["graph"], "solver_ctas": info["solver_ctas"],
+            "autotune_choice": choice, "mean_solver_iters": float(sum(its) / len(its))}
+
+
 def cpu_sample(n: int, seconds: float):
     """The oracle (f64, 1 thread) on the first steps of the same plume until
     `seconds` of CPU time have been spent."""
@@ -340,6 +385,13 @@ def run_ours(args):
     if not args.no_e2e:
         e2e = time_e2e(headline, args.n, args.steps, args.warmup, dist, torch)
 
+    ensemble = None
+    if not args.no_ensemble:
+        try:
+            ensemble = time_ensemble(args.ensemble_steps, torch)
+        except Exception as exc:  # reported, never hides the headline
+            ensemble = {"error": str(exc)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(args.n, args.cpu_seconds)
@@ -403,6 +455,7 @@ def run_ours(args):
                                     "k_cg_mixed") if headline == "mixed_cg" else headline,
                          "peak_source": peak_kind},
             "variants": variants,
+            "ensemble": ensemble,
             "adjoint_fwd_ratio": None,
         }
         if e2e:
