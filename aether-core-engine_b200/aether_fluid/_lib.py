@@ -151,6 +151,12 @@ SIGNATURES = [
     ("afl_ensemble_info", _st, [_vp, ctypes.POINTER(ctypes.c_int32)]),
     ("afl_ensemble_instance_ctas", _st, [_vp, ctypes.POINTER(ctypes.c_int32), _i]),
     ("afl_rng_f64", _st, [ctypes.c_uint64, ctypes.c_uint64, _sz, _dp]),
+    ("afl_adjoint_create", _st, [_sz, _sz, _sz, ctypes.POINTER(AflParams), _i,
+                                 ctypes.POINTER(_vp)]),
+    ("afl_adjoint_destroy", _st, [_vp]),
+    ("afl_adjoint_forward", _st, [_vp, _dp, _dp, _dp, _dp, _i, _d, _dp]),
+    ("afl_adjoint_backward", _st, [_vp, _dp, _dp, _dp, _dp, _dp]),
+    ("afl_adjoint_stats", _st, [_vp, _dp]),
     ("afl_solve_cg_noalloc", _st, [_vp, _vp, _sz, _sz, _sz, _i, _d, _vp,
                                     ctypes.POINTER(AflSolveInfo)]),
     ("afl_synchronize", _st, [_vp]),

@@ -292,6 +292,32 @@ afl_status afl_ensemble_instance_ctas(const afl_ensemble *e, int32_t *out, int c
  * skipping `skip` next_u64 draws from Rng::from_seed(seed). */
 afl_status afl_rng_f64(uint64_t seed, uint64_t skip, size_t n, double *out);
 
+/* ---- reverse mode (no reference counterpart) --------------------------------
+ * Gradient of a function of the final density with respect to the initial
+ * velocity and the per-cell temperature amplitude of the sphere source, through
+ * `steps` FP64 steps (sphere source, CG projection).  Hand-written adjoints of
+ * every stage; MacCormack clamp branches are recorded; the adjoint pressure
+ * solve uses the same symmetric-operator CG (solves treated as exact, so use a
+ * tight cg_rel_tol).  The state is checkpointed every `checkpoint_every` steps
+ * and each segment is recomputed during the backward pass. */
+typedef struct afl_adjoint afl_adjoint;
+/* params: source_kind must be AFL_SOURCE_SPHERE, solver_kind AFL_POISSON_CG. */
+afl_status afl_adjoint_create(size_t nx, size_t ny, size_t nz, const afl_params *params,
+                              int checkpoint_every, afl_adjoint **out);
+afl_status afl_adjoint_destroy(afl_adjoint *a);
+/* Host arrays of nx*ny*nz doubles; amp may be NULL (all 1); rho_final may be
+ * NULL.  Density, temperature and pressure start at zero. */
+afl_status afl_adjoint_forward(afl_adjoint *a, const double *u0, const double *v0,
+                               const double *w0, const double *amp, int steps, double dt,
+                               double *rho_final);
+/* rho_bar: the gradient of the function with respect to the final density.
+ * Any output may be NULL. */
+afl_status afl_adjoint_backward(afl_adjoint *a, const double *rho_bar, double *u0_bar,
+                                double *v0_bar, double *w0_bar, double *amp_bar);
+/* out = {last forward ms, last backward ms (recompute included), forward CG
+ * iterations, adjoint CG iterations} */
+afl_status afl_adjoint_stats(const afl_adjoint *a, double out[4]);
+
 /* ---- a pressure solve that allocates nothing --------------------------------
  * No counterpart in the reference.  For callers that may not allocate device
  * memory -- code recorded into a CUDA graph, real-time/render threads that

@@ -1,0 +1,157 @@
+"""Reverse mode through the FP64 smoke step: gradients of
+L = 0.5*sum((rho_final - rho_target)^2) with respect to the initial velocity
+and the source's temperature amplitude map, checked against central finite
+differences of the same forward, a dot-product test of the Jacobian, the
+checkpoint interval, and finite differences of the CPU oracle."""
+import numpy as np
+import pytest
+
+from helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+SHAPE = (20, 24, 18)
+STEPS = 6
+
+
+def wall_masked(u, v, w, shape):
+    """enforce_wall_velocity_bc (src/fluid.rs:236-253) on numpy arrays."""
+    nx, ny, nz = shape
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    ib = (i == 0) | (i + 1 >= nx)
+    jb = (j == 0) | (j + 1 >= ny)
+    kb = (k == 0) | (k + 1 >= nz)
+    mu = (i <= 1) | ib | jb | kb
+    mv = (j <= 1) | ib | jb | kb
+    mw = (k <= 1) | ib | jb | kb
+    return (np.where(mu.ravel(), 0.0, u), np.where(mv.ravel(), 0.0, v),
+            np.where(mw.ravel(), 0.0, w))
+
+
+def controls(shape, seed):
+    from aether_fluid.ensemble import rng_f64
+    nx, ny, nz = shape
+    n = nx * ny * nz
+    x = rng_f64(seed, 0, 4 * n)
+    u, v, w = (-0.01 + 0.02 * x[a * n:(a + 1) * n] for a in range(3))
+    u, v, w = wall_masked(u, v, w, shape)
+    amp = 0.5 + x[3 * n:]
+    return u, v, w, amp
+
+
+def source(shape, shift=0.0):
+    nx, ny, nz = shape
+    return (nx / 2 + shift, 0.1 * ny + 1.0, nz / 2), max(2.5, 5.0 * nx / 64.0)
+
+
+def make(af, shape, k=4, shift=0.0):
+    from aether_fluid.adjoint import Adjoint
+    c, r = source(shape, shift)
+    return Adjoint(*shape, center=c, radius=r, checkpoint_every=k)
+
+
+@pytest.fixture(scope="module")
+def case(af):
+    u, v, w, amp = controls(SHAPE, 5)
+    dt = 0.5 / max(SHAPE)
+    tgt = make(af, SHAPE, shift=3.0).forward(u, v, w, amp, STEPS, dt)
+    adj = make(af, SHAPE)
+    rho = adj.forward(u, v, w, amp, STEPS, dt)
+    grads = adj.backward(rho - tgt)
+    return {"x": (u, v, w, amp), "dt": dt, "tgt": tgt, "adj": adj, "rho": rho, "grads": grads}
+
+
+def loss(adj, x, dt, tgt):
+    rho = adj.forward(*x, STEPS, dt)
+    return 0.5 * float(np.sum((rho - tgt) ** 2))
+
+
+def directions(n, count, seed):
+    rng = np.random.default_rng(seed)
+    for _ in range(count):
+        d = [rng.standard_normal(n) for _ in range(4)]
+        nrm = np.sqrt(sum(float(np.dot(a, a)) for a in d))
+        yield [a / nrm for a in d]
+
+
+def test_gradient_matches_finite_differences(af, case):
+    adj, x, dt, tgt, g = case["adj"], case["x"], case["dt"], case["tgt"], case["grads"]
+    assert all(np.all(np.isfinite(a)) for a in g)
+    gnorm = np.sqrt(sum(float(np.dot(a, a)) for a in g))
+    assert gnorm > 0
+    eps = 1e-5
+    for d in directions(x[0].size, 6, 11):
+        lp = loss(adj, [a + eps * b for a, b in zip(x, d)], dt, tgt)
+        lm = loss(adj, [a - eps * b for a, b in zip(x, d)], dt, tgt)
+        fd = (lp - lm) / (2 * eps)
+        ad = sum(float(np.dot(a, b)) for a, b in zip(g, d))
+        assert abs(fd - ad) <= 1e-3 * max(abs(ad), 1e-3 * gnorm), (fd, ad)
+
+
+def test_dot_product(af, case):
+    """<J delta, w> (central differences of the final density) equals
+    <delta, J^T w> (one backward pass) for a random cotangent w."""
+    adj, x, dt = case["adj"], case["x"], case["dt"]
+    rng = np.random.default_rng(3)
+    wv = rng.standard_normal(x[0].size)
+    adj.forward(*x, STEPS, dt)
+    jtw = adj.backward(wv)
+    eps = 1e-5
+    for d in directions(x[0].size, 3, 17):
+        rp = adj.forward(*[a + eps * b for a, b in zip(x, d)], STEPS, dt)
+        rm = adj.forward(*[a - eps * b for a, b in zip(x, d)], STEPS, dt)
+        lhs = float(np.dot((rp - rm) / (2 * eps), wv))
+        rhs = sum(float(np.dot(a, b)) for a, b in zip(jtw, d))
+        assert abs(lhs - rhs) <= 1e-3 * max(abs(rhs), 1e-6), (lhs, rhs)
+
+
+@pytest.mark.parametrize("k", [1, 3, STEPS])
+def test_checkpoint_interval_does_not_change_the_gradient(af, case, k):
+    x, dt, tgt = case["x"], case["dt"], case["tgt"]
+    a = make(af, SHAPE, k=k)
+    rho = a.forward(*x, STEPS, dt)
+    assert np.array_equal(rho, case["rho"])
+    g = a.backward(rho - tgt)
+    for got, ref in zip(g, case["grads"]):
+        assert rel_l2(got, ref) <= 1e-9
+
+
+def test_forward_matches_oracle_and_oracle_fd(af, oracle, case):
+    """The adjoint's forward is the reference step (oracle to 1e-9), and the
+    adjoint gradient agrees with central differences of the f64 CPU oracle."""
+    O = oracle
+    x, dt, tgt, g = case["x"], case["dt"], case["tgt"], case["grads"]
+    c, r = source(SHAPE)
+
+    def oracle_rho(xx):
+        s = O.OracleSolver(*SHAPE)
+        s.set_params(vorticity_eps=0.3, buoyancy_beta=0.4, gravity_alpha=0.08,
+                     solver_kind=O.CG, solver_iters=2000, cg_rel_tol=1e-10)
+        for name, arr in zip(("u", "v", "w"), xx[:3]):
+            s.field(name)[:] = arr
+        s.set_sphere_source(c, r, 1.0, 1.0, temp_amp=xx[3])
+        for n in range(STEPS):
+            s.step(dt, n * dt)
+        return s.field("density").copy()
+
+    assert rel_l2(oracle_rho(x), case["rho"]) <= 1e-9
+    gnorm = np.sqrt(sum(float(np.dot(a, a)) for a in g))
+    eps = 1e-5
+    for d in directions(x[0].size, 2, 29):
+        lp = 0.5 * float(np.sum((oracle_rho([a + eps * b for a, b in zip(x, d)]) - tgt) ** 2))
+        lm = 0.5 * float(np.sum((oracle_rho([a - eps * b for a, b in zip(x, d)]) - tgt) ** 2))
+        fd = (lp - lm) / (2 * eps)
+        ad = sum(float(np.dot(a, b)) for a, b in zip(g, d))
+        assert abs(fd - ad) <= 1e-3 * max(abs(ad), 1e-3 * gnorm), (fd, ad)
+
+
+def test_torch_autograd_function(af, case):
+    import torch
+    from aether_fluid.adjoint import smoke_rollout
+    f = smoke_rollout()
+    x = [torch.tensor(a, dtype=torch.float64, requires_grad=True) for a in case["x"]]
+    rho = f.apply(*x, case["adj"], STEPS, case["dt"])
+    L = 0.5 * torch.sum((rho - torch.from_numpy(case["tgt"])) ** 2)
+    L.backward()
+    for t, ref in zip(x, case["grads"]):
+        assert rel_l2(t.grad.numpy(), ref) <= 1e-9
