@@ -65,6 +65,17 @@ class Adjoint:
         check(self._lib.afl_adjoint_backward(self._h, _p(rb), *[_p(o) for o in outs]))
         return tuple(outs)
 
+    def wall_masked(self, u, v, w):
+        """Copies of (u, v, w) with the wall-BC cells zeroed
+        (enforce_wall_velocity_bc, src/fluid.rs:236-253): the velocity
+        subspace every step leaves the state in."""
+        nx, ny, nz = self.nx, self.ny, self.nz
+        k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        edge = (i == 0) | (i + 1 >= nx) | (j == 0) | (j + 1 >= ny) | (k == 0) | (k + 1 >= nz)
+        masks = ((i <= 1) | edge, (j <= 1) | edge, (k <= 1) | edge)
+        return tuple(np.where(m.ravel(), 0.0, np.asarray(a, dtype=np.float64).ravel())
+                     for m, a in zip(masks, (u, v, w)))
+
     def stats(self) -> dict:
         out = (ctypes.c_double * 4)()
         check(self._lib.afl_adjoint_stats(self._h, out))
