@@ -30,7 +30,8 @@ struct PersistentState {
   unsigned int *count;
   unsigned int *gen;
   int *abort_flag;
-  double *partials;      // >= 6 * max_blocks doubles (2 buffers x 3 values)
+  double *partials;      // >= 12 * max_blocks doubles (streaming kernels: 2 buffers x 3
+                         // values; resident kernels: 2 buffers x 3 tagged values x 2 words)
   int max_blocks;
   unsigned long long timeout_ns;
 };

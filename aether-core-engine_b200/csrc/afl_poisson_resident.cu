@@ -50,18 +50,125 @@ __device__ __forceinline__ void bsum(double (&v)[NV], double *scratch) {
   for (int a = 0; a < NV; ++a) v[a] = scratch[kRW * NV + a];
 }
 
-// Fixed-order sum of NV interleaved per-CTA partials, read by warp 0 and
-// broadcast through `slot` (NV doubles); identical in every CTA.
+// ---- tagged partials: the grid-wide sums without a central barrier ---------
+// Every grid-wide sum of the solve is "each CTA contributes its partial, every
+// CTA needs the fixed-order total".  Instead of a counter barrier followed by
+// a read of the partials, each CTA stores its partial as two 64-bit words,
+// each carrying the number of the sum in its upper half and one half of the
+// double in its lower half (aligned 64-bit stores are single-copy atomic).
+// A reader polls a CTA's two words until both carry the expected number, so
+// arrival and data come in one L2 round trip and no CTA waits on an atomic.
+// Sum number k uses buffer k & 1: a CTA can publish sum k+1 only after it has
+// read all of sum k, and sum k+2 only after every CTA published k+1, so a
+// buffer is never rewritten while a CTA may still read it.  Tags start at 1;
+// the slots are zeroed before each launch.
+constexpr int kMaxNV = 3;
+
+struct TagSync {
+  unsigned long long *slots;  // 2 buffers x nblocks x 2*kMaxNV words
+  int nblocks;
+};
+
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long *tag_slot(const TagSync &ts, unsigned int tag,
+                                                       int block) {
+  return ts.slots + (static_cast<size_t>(tag & 1u) * ts.nblocks + block) * (2 * kMaxNV);
+}
+
+// Sums NV values over the CTA (warp butterflies, then warp 0 over the 32 warp
+// sums: a fixed order) and publishes the CTA's partials as sum number `tag`.
+// Writes made by any thread of the CTA before the call are released with it.
 template <int NV>
-__device__ __forceinline__ void reduce_parts(const double *parts, int nparts,
-                                             double (&out)[NV], double *slot) {
+__device__ __forceinline__ void tag_publish(const TagSync &ts, unsigned int tag,
+                                            double (&v)[NV], double *scratch) {
+  static_assert(NV <= kMaxNV, "too many values");
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < NV; ++a) v[a] = warp_sum(v[a]);
+  if (lane == 0)
+#pragma unroll
+    for (int a = 0; a < NV; ++a) scratch[warp * NV + a] = v[a];
+  __syncthreads();
+  if (warp == 0) {
+    double x[NV];
+#pragma unroll
+    for (int a = 0; a < NV; ++a) x[a] = warp_sum(scratch[lane * NV + a]);
+    if (lane == 0) {
+      unsigned long long *dst = tag_slot(ts, tag, blockIdx.x);
+      const unsigned long long hi_tag = static_cast<unsigned long long>(tag) << 32;
+      __threadfence();  // release: the CTA's writes before the sum (fence + relaxed stores)
+#pragma unroll
+      for (int a = 0; a < NV; ++a) {
+        const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(x[a]));
+        st_relaxed_u64(dst + 2 * a, hi_tag | (bits & 0xffffffffull));
+        st_relaxed_u64(dst + 2 * a + 1, hi_tag | (bits >> 32));
+      }
+    }
+  }
+}
+
+// The fixed-order total of sum number `tag` over all CTAs, in every thread.
+// Thread b waits for CTA b's words (relaxed loads; a fence after the wait
+// makes it an acquire of what CTA b released) and parks the value in shared
+// `vals`; then warp 0 lane l adds CTAs l, l+32, ... in that order and a
+// butterfly combines the lanes, so every CTA computes the same bits.  Waits
+// are bounded like grid_sync's (abort flag and clock polled every 256 spins; a
+// limit of 0 gives up at the first wait).  Returns false when a wait gave up;
+// the abort flag then holds the reason.
+constexpr int kMaxTagBlocks = 160;  // >= the SM count: one CTA per SM
+
+template <int NV>
+__device__ __forceinline__ bool tag_gather(const TagSync &ts, const GridSync &gs, unsigned int tag,
+                                           double (&out)[NV], double *slot, double *vals) {
+  int ok = 1;
+  const int b = threadIdx.x;
+  if (b < ts.nblocks) {
+    const unsigned long long *src = tag_slot(ts, tag, b);
+    unsigned long long w[2 * NV];
+    unsigned int spins = 0;
+    const unsigned long long t0 = global_ns();
+    for (;;) {
+      bool ready = true;
+#pragma unroll
+      for (int x = 0; x < 2 * NV; ++x) {
+        w[x] = ld_relaxed_u64(src + x);
+        ready &= static_cast<unsigned int>(w[x] >> 32) == tag;
+      }
+      if (ready) break;
+      if ((spins++ & 255u) == 0u) {
+        if (ld_relaxed_i32(gs.abort_flag) != 0) { ok = 0; break; }
+        if (gs.timeout_ns == 0 || global_ns() - t0 > gs.timeout_ns) {
+          atomicCAS(gs.abort_flag, 0, 1);
+          ok = 0;
+          break;
+        }
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < NV; ++a)
+      vals[b * NV + a] = __longlong_as_double(
+          static_cast<long long>((w[2 * a + 1] << 32) | (w[2 * a] & 0xffffffffull)));
+    // acquire: plain loads after the sum (halo values of other CTAs) must see
+    // the writes released with it
+    __threadfence();
+  }
+  ok = __syncthreads_and(ok);
   if (threadIdx.x < 32) {
     double acc[NV];
 #pragma unroll
     for (int a = 0; a < NV; ++a) acc[a] = 0.0;
-    for (int b = threadIdx.x; b < nparts; b += 32)
+    for (int bb = threadIdx.x; bb < ts.nblocks; bb += 32)
 #pragma unroll
-      for (int a = 0; a < NV; ++a) acc[a] += __ldcg(parts + b * NV + a);
+      for (int a = 0; a < NV; ++a) acc[a] += vals[bb * NV + a];
 #pragma unroll
     for (int a = 0; a < NV; ++a) {
       acc[a] = warp_sum(acc[a]);
@@ -71,27 +178,7 @@ __device__ __forceinline__ void reduce_parts(const double *parts, int nparts,
   __syncthreads();
 #pragma unroll
   for (int a = 0; a < NV; ++a) out[a] = slot[a];
-}
-
-// Sums NV values over the CTA (same fixed order as bsum) and stores the CTA's
-// partials to parts[blockIdx.x*NV + a]; only warp 0 sees the sum, so one CTA
-// barrier suffices (the grid barrier that follows starts with another).
-template <int NV>
-__device__ __forceinline__ void publish_sum(double *parts, double (&v)[NV], double *scratch) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int a = 0; a < NV; ++a) v[a] = warp_sum(v[a]);
-  if (lane == 0)
-#pragma unroll
-    for (int a = 0; a < NV; ++a) scratch[warp * NV + a] = v[a];
-  __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int a = 0; a < NV; ++a) {
-      const double x = warp_sum(scratch[lane * NV + a]);
-      if (lane == 0) parts[blockIdx.x * NV + a] = x;
-    }
-  }
+  return ok != 0;
 }
 
 // Where this thread's cells sit: column (ii, jj) of the tile, planes
@@ -152,11 +239,43 @@ struct Cells {
   }
 };
 
-// The reference operator (src/fluid.rs:356-394) on the shared-memory tile,
-// without branches: a missing neighbour contributes a selected 0 to the sum
-// (the reference skips it; the sum is the same value), the diagonal is the
-// count of present neighbours.  Shared slots of missing neighbours are never
-// used, whatever they hold.
+// The reference operator (src/fluid.rs:356-394) on the thread's column of
+// CPT cells, marching up in z with the z neighbours in registers.  No
+// branches or selects: a neighbour the reference skips is a cell outside the
+// interior, where the direction is exactly 0 (r = b - A p = 0 on every
+// non-interior cell, and d = r + beta*d keeps it 0), so adding it leaves the
+// neighbour sum's value unchanged; the sum keeps the reference's order
+// (x-, x+, y-, y+, z-, z+).  The diagonal is the count of interior
+// neighbours.  Only interior cells keep the result; their neighbours all lie
+// in the grid, so slots that hold no grid cell (halo outside the grid,
+// padding planes) never reach a kept result.
+// use(m, s, d_m, (A d)_m) is called for every cell of the column.
+template <typename R, int SX, int SXY, int CPT, typename Cl, typename F>
+__device__ __forceinline__ void lap_column(const Dims &g, const R *D, const Cl &cl, F &&use) {
+  int s = cl.s0;
+  R below = D[s - SXY];
+  R mid = D[s];
+#pragma unroll
+  for (int m = 0; m < CPT; ++m) {
+    const R above = D[s + SXY];
+    const int k = cl.k0 + m;
+    const int diag = cl.diag_xy + int(k > 1) + int(k + 2 < g.nz);
+    R nb = D[s - 1];
+    nb += D[s + 1];
+    nb += D[s - SX];
+    nb += D[s + SX];
+    nb += below;
+    nb += above;
+    use(m, s, mid, R(diag) * mid - nb);
+    below = mid;
+    mid = above;
+    s += SXY;
+  }
+}
+
+// The FP64 kernel's form of the same operator, one cell at a time with the
+// reference's neighbour tests as selects: its 16 f64 residuals per thread
+// leave too few registers for the column march above.
 template <typename R, int SX, int SXY, typename Cl>
 __device__ __forceinline__ R lap_smem(const Dims &g, const R *D, int s, const Cl &cl, int k) {
   const bool zl = k > 1, zh = k + 2 < g.nz;
@@ -230,11 +349,6 @@ struct Halo {
   }
 };
 
-struct Ring2 {
-  double *base;
-  int stride;
-  __device__ double *buf(int phase) const { return base + (phase & 1) * stride; }
-};
 
 // Shared scratch of the reductions: per-warp values, the CTA result, and the
 // broadcast slot of the grid-wide sums.
@@ -246,11 +360,12 @@ constexpr int kScratch = kRW * 3 + 3 + 3;
 // (updated once per iteration, never read by the operator).
 template <int TY, int CPT>
 __global__ void __launch_bounds__(kRT, 1)
-    k_cg_res_f64(ResidentCgArgs a, GridSync gs, Ring2 pr) {
+    k_cg_res_f64(ResidentCgArgs a, GridSync gs, TagSync ts) {
   using C = Cells<TY, CPT>;
   extern __shared__ double Dbase[];
   double *D = Dbase + C::SXY;  // one padding plane below plane 0
   __shared__ double scratch[kScratch];
+  __shared__ double vals[kMaxTagBlocks * kMaxNV];
   double *slot = scratch + kRW * 3 + 3;
   const Dims g = a.g;
   const C cl(g, a.tiles_x);
@@ -274,11 +389,10 @@ __global__ void __launch_bounds__(kRT, 1)
       acc[0] += rv * rv;
       acc[1] += bc * bc;
     }
-    publish_sum<2>(pr.buf(phase), acc, scratch);
+    tag_publish<2>(ts, unsigned(phase + 1), acc, scratch);
   }
-  if (!grid_sync(gs)) return;
   double tot[2];
-  reduce_parts<2>(pr.buf(phase), gridDim.x, tot, slot);
+  if (!tag_gather<2>(ts, gs, unsigned(phase + 1), tot, slot, vals)) return;
   ++phase;
   double delta = tot[0];
   const double bb = tot[1];
@@ -316,10 +430,9 @@ __global__ void __launch_bounds__(kRT, 1)
         const double qv = lap_smem<double, C::SX, C::SXY>(g, D, s, cl, cl.k0 + m);
         acc[0] += cl.interior(g, m) ? D[s] * qv : 0.0;
       }
-      publish_sum<1>(pr.buf(phase), acc, scratch);
-      if (!grid_sync(gs)) return;
+      tag_publish<1>(ts, unsigned(phase + 1), acc, scratch);
       double dq[1];
-      reduce_parts<1>(pr.buf(phase), gridDim.x, dq, slot);
+      if (!tag_gather<1>(ts, gs, unsigned(phase + 1), dq, slot, vals)) return;
       ++phase;
       if (fabs(dq[0]) < 1e-28) break;  // src/fluid.rs:469
       const double alpha = delta / dq[0];
@@ -337,10 +450,9 @@ __global__ void __launch_bounds__(kRT, 1)
         if (v && cl.edge) rpub[c] = rv;
         acc2[0] += rv * rv;
       }
-      publish_sum<1>(pr.buf(phase), acc2, scratch);
-      if (!grid_sync(gs)) return;
+      tag_publish<1>(ts, unsigned(phase + 1), acc2, scratch);
       double dn[1];
-      reduce_parts<1>(pr.buf(phase), gridDim.x, dn, slot);
+      if (!tag_gather<1>(ts, gs, unsigned(phase + 1), dn, slot, vals)) return;
       ++phase;
       ++it;
       last = dn[0];
@@ -365,23 +477,26 @@ __global__ void __launch_bounds__(kRT, 1)
 }
 
 // ---------------------------------------------------------------- mixed -----
-// f64 refinement around an f32 CG whose vectors never leave the SM: d and the
-// correction e in shared memory (same tile layout), r in registers.
+// f64 refinement around an f32 CG whose vectors never leave the SM: d and
+// q = A d in shared memory (same tile layout), r and the correction e in
+// registers.  q is stored by the first pass of an iteration and read by the
+// second, so the stencil runs once per iteration.
 template <int TY, int CPT>
 __global__ void __launch_bounds__(kRT, 1)
-    k_cg_res_mixed(ResidentCgArgs a, GridSync gs, Ring2 pr) {
+    k_cg_res_mixed(ResidentCgArgs a, GridSync gs, TagSync ts) {
   using C = Cells<TY, CPT>;
   extern __shared__ float Dfbase[];
   float *Df = Dfbase + C::SXY;  // one padding plane below plane 0
   __shared__ double scratch[kScratch];
+  __shared__ double vals[kMaxTagBlocks * kMaxNV];
   double *slot = scratch + kRW * 3 + 3;
   const Dims g = a.g;
   const C cl(g, a.tiles_x);
   const Halo<TY> halo(g, a.tiles_x);
-  float *E = Df + C::SXY * (C::kPlanes + 2);  // the correction, same tile layout
+  float *Q = Df + C::SXY * (C::kPlanes + 2);  // q = A d, same tile layout
   double *p = a.p;
   float *rpub = static_cast<float *>(a.rpub);
-  float r[CPT];
+  float r[CPT], e[CPT];
   int phase = 0;
 
   // r = b - A p in f64, rounded once to f32; e = 0.
@@ -390,7 +505,7 @@ __global__ void __launch_bounds__(kRT, 1)
 #pragma unroll
     for (int m = 0; m < CPT; ++m) {
       r[m] = 0.0f;
-      E[cl.s0 + m * C::SXY] = 0.0f;
+      e[m] = 0.0f;
       if (!cl.valid(g, m)) continue;
       const int c = cl.c0 + m * g.nxy;
       const double ap = cl.interior(g, m) ? lap_global(g, p, c, cl.i, cl.j, cl.k0 + m) : 0.0;
@@ -403,13 +518,12 @@ __global__ void __launch_bounds__(kRT, 1)
       if (with_b) acc[1] += bc * bc;
       acc[2] += double(rf) * double(rf);
     }
-    publish_sum<3>(pr.buf(phase), acc, scratch);
+    tag_publish<3>(ts, unsigned(phase + 1), acc, scratch);
   };
 
   outer_residual(true);
-  if (!grid_sync(gs)) return;
   double tot[3];
-  reduce_parts<3>(pr.buf(phase), gridDim.x, tot, slot);
+  if (!tag_gather<3>(ts, gs, unsigned(phase + 1), tot, slot, vals)) return;
   ++phase;
   const double bb = tot[1];
   double rr = tot[0];
@@ -443,16 +557,14 @@ __global__ void __launch_bounds__(kRT, 1)
       });
       __syncthreads();
       double acc[1] = {0.0};
-#pragma unroll
-      for (int m = 0; m < CPT; ++m) {
-        const int s = cl.s0 + m * C::SXY;
-        const float qv = lap_smem<float, C::SX, C::SXY>(g, Df, s, cl, cl.k0 + m);
-        acc[0] += cl.interior(g, m) ? double(Df[s]) * double(qv) : 0.0;
-      }
-      publish_sum<1>(pr.buf(phase), acc, scratch);
-      if (!grid_sync(gs)) return;
+      lap_column<float, C::SX, C::SXY, CPT>(g, Df, cl, [&](int m, int s, float dv, float lq) {
+        const float qv = cl.interior(g, m) ? lq : 0.0f;
+        Q[s] = qv;
+        acc[0] += double(dv) * double(qv);
+      });
+      tag_publish<1>(ts, unsigned(phase + 1), acc, scratch);
       double dq[1];
-      reduce_parts<1>(pr.buf(phase), gridDim.x, dq, slot);
+      if (!tag_gather<1>(ts, gs, unsigned(phase + 1), dq, slot, vals)) return;
       ++phase;
       if (!(fabs(dq[0]) >= 1e-30)) break;
       const float af = float(delta / dq[0]);
@@ -460,18 +572,16 @@ __global__ void __launch_bounds__(kRT, 1)
 #pragma unroll
       for (int m = 0; m < CPT; ++m) {
         const int s = cl.s0 + m * C::SXY;
-        const float lq = lap_smem<float, C::SX, C::SXY>(g, Df, s, cl, cl.k0 + m);
-        const float qv = cl.interior(g, m) ? lq : 0.0f;
-        E[s] = __fmaf_rn(af, Df[s], E[s]);
+        const float qv = Q[s];
+        e[m] = __fmaf_rn(af, Df[s], e[m]);
         const float rv = __fmaf_rn(-af, qv, r[m]);
         r[m] = rv;
         if (cl.edge && cl.valid(g, m)) rpub[cl.c0 + m * g.nxy] = rv;
         acc2[0] += double(rv) * double(rv);
       }
-      publish_sum<1>(pr.buf(phase), acc2, scratch);
-      if (!grid_sync(gs)) return;
+      tag_publish<1>(ts, unsigned(phase + 1), acc2, scratch);
       double dn[1];
-      reduce_parts<1>(pr.buf(phase), gridDim.x, dn, slot);
+      if (!tag_gather<1>(ts, gs, unsigned(phase + 1), dn, slot, vals)) return;
       ++phase;
       ++it;
       ++total;
@@ -484,12 +594,11 @@ __global__ void __launch_bounds__(kRT, 1)
     for (int m = 0; m < CPT; ++m) {
       if (!cl.valid(g, m)) continue;
       const int c = cl.c0 + m * g.nxy;
-      p[c] = p[c] + double(E[cl.s0 + m * C::SXY]);
+      p[c] = p[c] + double(e[m]);
     }
     if (!grid_sync(gs)) return;
     outer_residual(false);
-    if (!grid_sync(gs)) return;
-    reduce_parts<3>(pr.buf(phase), gridDim.x, tot, slot);
+    if (!tag_gather<3>(ts, gs, unsigned(phase + 1), tot, slot, vals)) return;
     ++phase;
     rr = tot[0];
     ++passes;
@@ -509,7 +618,7 @@ __global__ void __launch_bounds__(kRT, 1)
 }
 
 // ---------------------------------------------------------------- dispatch --
-using KernelFn = void (*)(ResidentCgArgs, GridSync, Ring2);
+using KernelFn = void (*)(ResidentCgArgs, GridSync, TagSync);
 
 template <int TY, int CPT>
 KernelFn pick_kernel(bool f64) {
@@ -530,7 +639,7 @@ KernelFn kernel_for(bool f64, int ty, int cpt) {
 }  // namespace
 
 size_t resident_smem_bytes(const Dims &g, int ty, int cpt, bool f64) {
-  // FP64: the direction tile.  Mixed: direction and correction tiles (f32).
+  // FP64: the direction tile.  Mixed: direction and q = A d tiles (f32).
   // Planes: those the threads cover (groups*cpt >= nz) plus one padding plane
   // on each side, so every shared access of the branch-free loops is in bounds.
   (void)g;
@@ -545,7 +654,7 @@ bool plan_resident(const Dims &g, bool f64, ResidentPlan *plan) {
   if (cudaGetDevice(&dev) != cudaSuccess) return false;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const size_t static_smem = 2048;  // reduction scratch + barrier flag, rounded up
+  const size_t static_smem = 6144;  // reduction scratch, tagged-sum values, flags, rounded up
   bool found = false;
   ResidentPlan best{};
   for (int ty : {4, 8, 16}) {
@@ -557,7 +666,7 @@ bool plan_resident(const Dims &g, bool f64, ResidentPlan *plan) {
     const int tiles_x = (g.nx + kTX - 1) / kTX;
     const int tiles_y = (g.ny + ty - 1) / ty;
     const int tiles = tiles_x * tiles_y;
-    if (tiles > sms) continue;
+    if (tiles > sms || tiles > kMaxTagBlocks) continue;
     const size_t smem = resident_smem_bytes(g, ty, rounded, f64);
     if (smem + static_smem > static_cast<size_t>(smem_optin)) continue;
     ResidentPlan cand{ty, rounded, tiles_x, tiles_y, static_cast<int>(smem)};
@@ -593,8 +702,10 @@ int launch_cg_resident(const ResidentCgArgs &a, const ResidentPlan &plan, bool f
   gs.abort_flag = ps.abort_flag;
   gs.nblocks = static_cast<unsigned int>(blocks);
   gs.timeout_ns = ps.timeout_ns;
-  Ring2 pr{ps.partials, 3 * ps.max_blocks};
-  void *params[] = {&args, &gs, &pr};
+  // the tagged-partial slots (2 buffers x blocks x 2*kMaxNV words) start at 0
+  TagSync ts{reinterpret_cast<unsigned long long *>(ps.partials), blocks};
+  cudaMemsetAsync(ts.slots, 0, sizeof(unsigned long long) * 2 * kMaxNV * 2 * blocks, st);
+  void *params[] = {&args, &gs, &ts};
   err = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(fn), dim3(blocks), dim3(kRT),
                                     params, static_cast<size_t>(plan.smem_bytes), st);
   return err == cudaSuccess ? blocks : -static_cast<int>(err);

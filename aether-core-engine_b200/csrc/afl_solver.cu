@@ -629,7 +629,7 @@ afl_status afl_create(size_t nx, size_t ny, size_t nz, const afl_params *params,
     s->ps.count = bar;
     s->ps.gen = bar + 1;
     s->ps.abort_flag = reinterpret_cast<int *>(bar + 2);
-    st = alloc_as(s, &s->ps.partials, sizeof(double) * 6 * static_cast<size_t>(maxb));
+    st = alloc_as(s, &s->ps.partials, sizeof(double) * 12 * static_cast<size_t>(maxb));
   }
   if (st == AFL_OK && cudaMallocHost(&s->h_scal, sizeof(double) * 16) != cudaSuccess)
     st = set_error(AFL_ERR_OUT_OF_MEMORY, "cudaMallocHost failed");
