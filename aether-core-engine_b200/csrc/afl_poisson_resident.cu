@@ -336,15 +336,32 @@ struct Halo {
     col_c = j * g.nx + i;
     col_s = (jj + 1) * SX + ii + 1;
   }
-  // D[ring cell] = value_at(global cell, D[ring cell]) for every plane.
+  // D[ring cell] = value_at(global cell, D[ring cell]) for every plane.  The
+  // trip count is a constant (the planes the tile covers), so every L2 load of
+  // the ring is issued before the first use.
+  // The FP64 kernel's form: a rolled loop (its registers are taken by the
+  // f64 residuals).
   template <typename R, typename F>
-  __device__ __forceinline__ void fill(const Dims &g, R *D, const F &value_at) const {
+  __device__ __forceinline__ void fill_rolled(const Dims &g, R *D, const F &value_at) const {
     constexpr int SXY = Plane<TY>::SXY;
     if (!active) return;
 #pragma unroll 4
     for (int k = k_first; k < g.nz; k += kLanes) {
       R &slot = D[k * SXY + col_s];
       slot = value_at(k * g.nxy + col_c, slot);
+    }
+  }
+  template <int kTrips, typename R, typename F>
+  __device__ __forceinline__ void fill(const Dims &g, R *D, const F &value_at) const {
+    constexpr int SXY = Plane<TY>::SXY;
+    if (!active) return;
+#pragma unroll
+    for (int t = 0; t < kTrips; ++t) {
+      const int k = k_first + t * kLanes;
+      if (k < g.nz) {
+        R &slot = D[k * SXY + col_s];
+        slot = value_at(k * g.nxy + col_c, slot);
+      }
     }
   }
 };
@@ -418,7 +435,7 @@ __global__ void __launch_bounds__(kRT, 1)
         const int s = cl.s0 + m * C::SXY;
         D[s] = first ? r[m] : r[m] + beta * D[s];
       }
-      halo.fill(g, D, [&](int c, double dprev) {
+      halo.fill_rolled(g, D, [&](int c, double dprev) {
         const double rv = __ldcg(rpub + c);
         return first ? rv : rv + beta * dprev;
       });
@@ -485,6 +502,7 @@ template <int TY, int CPT>
 __global__ void __launch_bounds__(kRT, 1)
     k_cg_res_mixed(ResidentCgArgs a, GridSync gs, TagSync ts) {
   using C = Cells<TY, CPT>;
+  constexpr int kRingTrips = (C::kPlanes + Halo<TY>::kLanes - 1) / Halo<TY>::kLanes;
   extern __shared__ float Dfbase[];
   float *Df = Dfbase + C::SXY;  // one padding plane below plane 0
   __shared__ double scratch[kScratch];
@@ -546,15 +564,15 @@ __global__ void __launch_bounds__(kRT, 1)
     while (it < a.max_inner && total < a.max_iters) {
       const bool first = it == 0;
       const float bf = float(beta);
+      halo.template fill<kRingTrips>(g, Df, [&](int c, float dprev) {
+        const float rv = __ldcg(rpub + c);
+        return first ? rv : __fmaf_rn(bf, dprev, rv);
+      });
 #pragma unroll
       for (int m = 0; m < CPT; ++m) {
         const int s = cl.s0 + m * C::SXY;
         Df[s] = first ? r[m] : __fmaf_rn(bf, Df[s], r[m]);
       }
-      halo.fill(g, Df, [&](int c, float dprev) {
-        const float rv = __ldcg(rpub + c);
-        return first ? rv : __fmaf_rn(bf, dprev, rv);
-      });
       __syncthreads();
       double acc[1] = {0.0};
       lap_column<float, C::SX, C::SXY, CPT>(g, Df, cl, [&](int m, int s, float dv, float lq) {

@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the 48-plume batched-ensemble measurement")
     ap.add_argument("--ensemble-steps", type=int, default=100)
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the 256^3 x 100-step mixed/FP64 measurement")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the reverse-mode (adjoint) measurement")
     ap.add_argument("--adjoint-directions", type=int, default=16,
@@ -78,11 +80,12 @@ SEED = 0
 POISSON_KERNEL = 0
 
 
-def plume_for(form: str, n: int):
+def plume_for(form: str, n: int, seed: int | None = None):
     from aether_fluid.plume import Plume
+    seed = SEED if seed is None else seed
     if form.endswith("sor"):
-        return Plume(n, n, n, 200, seed=SEED, solver="sor", iters=80)
-    return Plume(n, n, n, 200, seed=SEED)
+        return Plume(n, n, n, 200, seed=seed, solver="sor", iters=80)
+    return Plume(n, n, n, 200, seed=seed)
 
 
 # ---------------------------------------------------------------- clocks -----
@@ -175,6 +178,55 @@ def step_bytes(n_cells: int, form: str, infos) -> float:
     return total * n_cells
 
 
+# Algorithmic bytes per cell of each timed stage (each stage reads each distinct
+# input array once and writes each output once, at its stored precision;
+# intermediates count 0): advect = u, v, w, density and temperature;
+# forces = confinement + buoyancy + wall BC; telemetry is counted as fused
+# into the scalar advection (0 bytes of its own).
+STAGE_BYTES = {"fp64": {"advect": 96 + 56, "forces": 64, "divergence": 32, "project": 56},
+               "mixed": {"advect": 48 + 28, "forces": 32, "divergence": 20, "project": 32}}
+
+
+def stage_fractions(form: str, cells: int, r: dict, peak: float) -> dict:
+    """Per stage: algorithmic GB/s over the stage's event-timed duration, as a
+    fraction of the measured HBM peak; the Poisson stage uses the solver
+    reports' iteration counts."""
+    kind = "mixed" if form.startswith("mixed") else "fp64"
+    steps = len(r["infos"])
+    out = {}
+    for stage, per_cell in STAGE_BYTES[kind].items():
+        ms = r["stages"][stage][0]
+        if ms > 0:
+            out[stage] = per_cell * cells * steps / (ms / 1e3) / 1e9 / peak
+    pms = r["stages"]["poisson"][0]
+    if pms > 0:
+        out["poisson"] = poisson_bytes(cells, form, r["infos"]) / (pms / 1e3) / 1e9 / peak
+    return out
+
+
+def time_large(torch, n: int = 256, steps: int = 100, seed: int = 1) -> dict:
+    """The 256^3 x 100-step plume (seed 1, source (128, 25.6, 128) r = 20) in
+    the mixed and FP64 CG forms: throughput, whole-step and per-stage fractions
+    of the measured HBM peak (state far larger than L2), and the mixed/FP64
+    ratio."""
+    peak, _ = measured_peak()
+    out = {"grid": [n, n, n], "steps": steps, "seed": seed}
+    for form in ("mixed_cg", "fp64_cg"):
+        r = time_form(form, n, steps, 3, None, torch, 0, seed=seed)
+        cells = r["cells"]
+        its = [i.iterations for i in r["infos"]]
+        out[form] = {"value": cells * steps / (r["ms"] / 1e3) / 1e6,
+                     "ms_per_step": r["ms"] / steps,
+                     "mean_solver_iters": sum(its) / len(its),
+                     "step_roofline_frac": step_bytes(cells, form, r["infos"]) / (r["ms"] / 1e3)
+                     / 1e9 / peak,
+                     "stage_roofline_frac": stage_fractions(form, cells, r, peak),
+                     "stage_ms": {k: round(v[0], 3) for k, v in r["stages"].items()},
+                     "poisson_plan": r["plan"]}
+    out["mixed_over_fp64"] = out["mixed_cg"]["value"] / out["fp64_cg"]["value"]
+    return out
+
+
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -185,9 +237,15 @@ def measured_peak():
 
 
 # ---------------------------------------------------------------- our arm ----
-def time_form(form: str, n: int, steps: int, warmup: int, dist, torch, rank: int):
+def time_form(form: str, n: int, steps: int, warmup: int, dist, torch, rank: int,
+              seed: int | None = None):
+    """K steps of one form from the initial state, timed on the solver's
+    stream with CUDA events (barrier + synchronize on both sides).  A second,
+    identical pass with per-stage CUDA events gives the stage breakdown and the
+    Poisson kernel's time for the roofline; it is kept out of the headline
+    because the extra events cost a few per cent of a step."""
     import aether_fluid as af
-    p = plume_for(form, n)
+    p = plume_for(form, n, seed)
     s = p.build(precision=af.Precision.MIXED if form.startswith("mixed") else af.Precision.FP64)
     s.set_params(poisson_kernel=POISSON_KERNEL)
     if warmup > 0:
@@ -197,7 +255,6 @@ def time_form(form: str, n: int, steps: int, warmup: int, dist, torch, rank: int
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
     plan = s.poisson_plan()
-    s.set_stage_timing(True)
     launches0 = s.launch_count()
     if dist:
         dist.barrier()
@@ -210,9 +267,15 @@ def time_form(form: str, n: int, steps: int, warmup: int, dist, torch, rank: int
         dist.barrier()
     ms = start.elapsed_time(end)
     launches = s.launch_count() - launches0
+    fields = {f: s.get_field(f) for f in ("u", "v", "w", "density", "temperature")}
+    # the stage breakdown: the same K steps again, with per-stage events
+    s.init_velocity_noise(p.seed)
+    s.set_stage_timing(True)
+    torch.cuda.synchronize()
+    s.run(steps, p.dt, 0.0, p.dt)
+    torch.cuda.synchronize()
     stages = s.stage_timing()
     s.set_stage_timing(False)
-    fields = {f: s.get_field(f) for f in ("u", "v", "w", "density", "temperature")}
     s.close()
     return {"ms": ms, "infos": infos, "tel": tel, "stages": stages, "launches": launches,
             "fields": fields, "cells": p.cells, "plan": plan}
@@ -460,6 +523,13 @@ def run_ours(args):
         except Exception as exc:  # reported, never hides the headline
             ensemble = {"error": str(exc)}
 
+    large = None
+    if not args.no_large and rank == 0:
+        try:
+            large = time_large(torch)
+        except Exception as exc:  # reported, never hides the headline
+            large = {"error": str(exc)}
+
     adjoint = None
     if not args.no_adjoint:
         try:
@@ -491,6 +561,7 @@ def run_ours(args):
                 "max_solver_iters": int(np.max(its)),
                 "converged_steps": int(sum(i.converged for i in r["infos"])),
                 "step_roofline_frac": sb / (r["ms"] / 1e3) / 1e9 / peak,
+                "stage_roofline_frac": stage_fractions(form, cells, r, peak),
                 "stage_ms": {k: round(v[0], 3) for k, v in r["stages"].items()},
                 "poisson_plan": r["plan"] if "cg" in form else None,
             }
@@ -530,6 +601,7 @@ def run_ours(args):
                                     "k_cg_mixed") if headline == "mixed_cg" else headline,
                          "peak_source": peak_kind},
             "variants": variants,
+            "large_256": large,
             "ensemble": ensemble,
             "adjoint_fwd_ratio": adjoint.get("adjoint_fwd_ratio") if adjoint else None,
             "adjoint": adjoint,
