@@ -227,6 +227,14 @@ def time_large(torch, n: int = 256, steps: int = 100, seed: int = 1) -> dict:
     return out
 
 
+# DRAM bytes per launch of the Poisson kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum from one ncu capture of the same workload:
+# profiles/k_cg_res_plume128.md and profiles/k_cg_stream_plume256.md).  Keyed by
+# (form, grid edge, resident kernel); other workloads report null.
+NCU_TRAFFIC = {("mixed_cg", 128, True): 42.9e6, ("fp64_cg", 128, True): 148.5e6,
+               ("mixed_cg", 256, False): 135.93e9, ("fp64_cg", 256, False): 268.68e9}
+
+
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -329,46 +337,55 @@ def time_e2e(form: str, n: int, steps: int, warmup: int, dist, torch):
     return {"seconds": el, "h2d_per_step": h2d / steps, "d2h_per_step": d2h / steps}
 
 
-def time_ensemble(steps: int, torch):
-    """The 48-plume ensemble (mixed CG to 1e-6): one batched, graph-captured
-    run of `steps` steps against the same 48 plumes run one at a time through
-    single-grid solvers.  Device time; states start from the initial
-    condition."""
+def time_ensemble(steps: int, torch, dist=None):
+    """The 48-plume ensemble (mixed CG to 1e-6) through the sharded-ensemble
+    API: each rank advances a cell-balanced share of the instances as one
+    batched, graph-captured ensemble on its GPU (no data-path collective; a
+    host-side gather returns the results to rank 0).  Whole-job time is the
+    slowest rank's.  At one GPU the same 48 plumes also run one at a time
+    through single-grid solvers, for comparison."""
     import aether_fluid as af
-    from aether_fluid.ensemble import Ensemble, plume48
+    from aether_fluid.ensemble import plume48
+    from aether_fluid.sharding import run_sharded
     specs = plume48()
     cells = sum(s.cells for s in specs)
-    ens = Ensemble(specs, precision=af.Precision.MIXED)
-    choice = ens.autotune()
-    info = ens.info()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    _, infos = ens.run(steps)
-    torch.cuda.synchronize()
-    batched = time.perf_counter() - t0
+    if dist:
+        dist.barrier()
+    res = run_sharded(specs, steps, dist=dist, precision=af.Precision.MIXED)
+    world = dist.get_world_size() if dist else 1
+    if res is None:                      # ranks other than 0
+        return None
+    _, infos, parts = res
+    batched = max(p.get("run_seconds", 0.0) for p in parts)
     its = [i.iterations for row in infos for i in row]
-    ens.close()
-    single_s = 0.0
-    for sp in specs:
-        s = af.FluidSolver3D(sp.nx, sp.ny, sp.nz, precision=af.Precision.MIXED)
-        s.set_params(vorticity_eps=sp.eps, buoyancy_beta=sp.beta, gravity_alpha=sp.alpha,
-                     solver_kind=0, solver_iters=200, cg_rel_tol=1e-6)
-        s.init_velocity_noise(sp.seed, -sp.noise, sp.noise)
-        s.set_sphere_source(sp.center, sp.radius)
-        s.run(1, sp.dt)                 # warm the kernels (untimed)
-        s.init_velocity_noise(sp.seed, -sp.noise, sp.noise)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        s.run(steps, sp.dt, 0.0, sp.dt)
-        torch.cuda.synchronize()
-        single_s += time.perf_counter() - t0
-        s.close()
-    return {"instances": len(specs), "cells": cells, "steps": steps,
-            "batched_mcell_steps_per_s": cells * steps / batched / 1e6,
-            "one_at_a_time_mcell_steps_per_s": cells * steps / single_s / 1e6,
-            "speedup": single_s / batched, "batched_s": batched, "one_at_a_time_s": single_s,
-            "graph": info["graph"], "solver_ctas": info["solver_ctas"],
-            "autotune_choice": choice, "mean_solver_iters": float(sum(its) / len(its))}
+    out = {"instances": len(specs), "cells": cells, "steps": steps, "ranks": world,
+           "batched_mcell_steps_per_s": cells * steps / batched / 1e6,
+           "batched_s": batched, "mean_solver_iters": float(sum(its) / len(its)),
+           "per_rank": [{"rank": p["rank"], "instances": len(p["indices"]),
+                         "cells": p.get("cells", 0), "run_s": p.get("run_seconds"),
+                         "graph": p.get("info", {}).get("graph"),
+                         "solver_ctas": p.get("info", {}).get("solver_ctas"),
+                         "autotune_choice": p.get("autotune_choice")} for p in parts]}
+    if world == 1:
+        single_s = 0.0
+        for sp in specs:
+            s = af.FluidSolver3D(sp.nx, sp.ny, sp.nz, precision=af.Precision.MIXED)
+            s.set_params(vorticity_eps=sp.eps, buoyancy_beta=sp.beta, gravity_alpha=sp.alpha,
+                         solver_kind=0, solver_iters=200, cg_rel_tol=1e-6)
+            s.init_velocity_noise(sp.seed, -sp.noise, sp.noise)
+            s.set_sphere_source(sp.center, sp.radius)
+            s.run(1, sp.dt)                 # warm the kernels (untimed)
+            s.init_velocity_noise(sp.seed, -sp.noise, sp.noise)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.run(steps, sp.dt, 0.0, sp.dt)
+            torch.cuda.synchronize()
+            single_s += time.perf_counter() - t0
+            s.close()
+        out["one_at_a_time_mcell_steps_per_s"] = cells * steps / single_s / 1e6
+        out["one_at_a_time_s"] = single_s
+        out["speedup"] = single_s / batched
+    return out
 
 
 def time_adjoint(ndir: int, torch, n: int = 96, steps: int = 64, every: int = 8):
@@ -519,7 +536,7 @@ def run_ours(args):
     ensemble = None
     if not args.no_ensemble:
         try:
-            ensemble = time_ensemble(args.ensemble_steps, torch)
+            ensemble = time_ensemble(args.ensemble_steps, torch, dist)
         except Exception as exc:  # reported, never hides the headline
             ensemble = {"error": str(exc)}
 
@@ -596,9 +613,19 @@ def run_ours(args):
                        "l2": "state larger than L2 (no flush between steps)"},
             "gpu_launches": int(head["launches"]),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "kernel": ("k_cg_res_mixed" if head["plan"]["resident"] else
-                                    "k_cg_mixed") if headline == "mixed_cg" else headline,
+                         "frac": achieved / peak,
+                         "traffic": NCU_TRAFFIC.get((headline, args.n,
+                                                     bool(head["plan"]["resident"]))),
+                         "algorithmic_bytes_per_launch": pois_bytes / pois_calls,
+                         "kernel": {"mixed_cg": ("k_cg_res_mixed", "k_cg_stream_mixed"),
+                                    "fp64_cg": ("k_cg_res_f64", "k_cg_stream_f64"),
+                                    "fp64_sor": ("k_rbsor_f64",) * 2,
+                                    "mixed_sor": ("k_rbsor_mixed",) * 2}[headline][
+                                        0 if head["plan"]["resident"] else 1],
+                         "note": ("on-chip resident solve: achieved is algorithmic bytes over "
+                                  "kernel time (an effective bandwidth); DRAM traffic is the "
+                                  "measured ncu figure" if head["plan"]["resident"] else
+                                  "streaming solve through HBM"),
                          "peak_source": peak_kind},
             "variants": variants,
             "large_256": large,

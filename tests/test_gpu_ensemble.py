@@ -86,3 +86,18 @@ def test_plume48_runs(af):
         for m in range(48):
             i = infos[n][m]
             assert i.final_residual < i.initial_residual, (n, m, i)
+
+
+def test_sharded_api_single_rank_is_the_batched_ensemble(af):
+    """run_sharded with one process runs the whole list as one ensemble: the
+    gathered telemetry is the ensemble's, in the original instance order."""
+    from aether_fluid.ensemble import Ensemble
+    from aether_fluid.sharding import run_sharded
+    specs = specs_small()
+    tel, infos, parts = run_sharded(specs, 3, dist=None, precision=0, autotune=False)
+    assert parts[0]["indices"] == list(range(len(specs)))
+    assert parts[0]["run_seconds"] > 0
+    ref_tel, ref_infos = Ensemble(specs, precision=0).run(3)
+    np.testing.assert_array_equal(tel, ref_tel)
+    assert [[i.iterations for i in row] for row in infos] == \
+        [[i.iterations for i in row] for row in ref_infos]
