@@ -37,7 +37,7 @@ struct PersistentState {
 };
 
 // Number of CTAs the reduction kernels use (fixed, so sums are reproducible).
-constexpr int kReduceBlocks = 592;  // 4 per SM on a 148-SM B200
+constexpr int kReduceBlocks = 1184;  // 8 per SM on a 148-SM B200 (full occupancy at 256 threads)
 constexpr int kReduceMaxVals = 8;
 
 template <typename T>

@@ -28,6 +28,25 @@ __device__ __forceinline__ bool cell_of_thread(const Dims &g, int &i, int &j, in
   return i < g.nx && j < g.ny;
 }
 
+// The forward stage kernels give each thread kKz consecutive z planes of its
+// (i, j) column: independent cells, so their loads are in flight together.
+constexpr int kKz = 2;
+inline dim3 column_grid(const Dims &g) {
+  return dim3((g.nx + kTx - 1) / kTx, (g.ny + kTy - 1) / kTy, (g.nz + kKz - 1) / kKz);
+}
+
+// Runs body(i, j, k) for the thread's cells of a column_grid launch.
+template <typename F>
+__device__ __forceinline__ void for_column_cells(const Dims &g, F &&body) {
+  const int i = blockIdx.x * kTx + threadIdx.x;
+  const int j = blockIdx.y * kTy + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const int k0 = blockIdx.z * kKz;
+#pragma unroll
+  for (int t = 0; t < kKz; ++t)
+    if (k0 + t < g.nz) body(i, j, k0 + t);
+}
+
 // Each stage is a per-cell device function (shared by the single-grid kernels
 // below and the batched ensemble kernels of afl_ensemble.cu, so both run the
 // same arithmetic) plus a thin kernel over one grid.
@@ -56,9 +75,9 @@ __global__ void __launch_bounds__(kTx *kTy)
     k_advect_fwd(Dims g, const T *__restrict__ u, const T *__restrict__ v,
                  const T *__restrict__ w, const T *__restrict__ src, T *__restrict__ fwd,
                  T scale) {
-  int i, j, k;
-  if (!cell_of_thread(g, i, j, k)) return;
-  cell_advect_fwd(g, u, v, w, src, fwd, scale, i, j, k);
+  for_column_cells(g, [&](int i, int j, int k) {
+    cell_advect_fwd(g, u, v, w, src, fwd, scale, i, j, k);
+  });
 }
 
 // Pass 2: the reference's bwd = SL(fwd, -dt) (:184) is evaluated on the fly at
@@ -109,21 +128,21 @@ __global__ void __launch_bounds__(kTx *kTy)
                 const T *__restrict__ w, const T *__restrict__ src,
                 const T *__restrict__ fwd, T *__restrict__ out, T scale_f, T scale_b,
                 T dissipation, int nonneg) {
-  int i, j, k;
-  if (!cell_of_thread(g, i, j, k)) return;
-  cell_advect_mc(g, u, v, w, src, fwd, out, scale_f, scale_b, dissipation, nonneg, i, j, k);
+  for_column_cells(g, [&](int i, int j, int k) {
+    cell_advect_mc(g, u, v, w, src, fwd, out, scale_f, scale_b, dissipation, nonneg, i, j, k);
+  });
 }
 
 // ---- enforce_wall_velocity_bc (src/fluid.rs:236-253) -----------------------
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
     k_wall_bc(Dims g, T *__restrict__ u, T *__restrict__ v, T *__restrict__ w) {
-  int i, j, k;
-  if (!cell_of_thread(g, i, j, k)) return;
-  const int c = (k * g.ny + j) * g.nx + i;
-  if (wall_u(g, i, j, k)) u[c] = T(0);
-  if (wall_v(g, i, j, k)) v[c] = T(0);
-  if (wall_w(g, i, j, k)) w[c] = T(0);
+  for_column_cells(g, [&](int i, int j, int k) {
+    const int c = (k * g.ny + j) * g.nx + i;
+    if (wall_u(g, i, j, k)) u[c] = T(0);
+    if (wall_v(g, i, j, k)) v[c] = T(0);
+    if (wall_w(g, i, j, k)) w[c] = T(0);
+  });
 }
 
 // ---- vorticity confinement + buoyancy (src/fluid.rs:256-330) ---------------
@@ -163,9 +182,9 @@ __global__ void __launch_bounds__(kTx *kTy)
     k_curl(Dims g, const T *__restrict__ u, const T *__restrict__ v,
            const T *__restrict__ w, T *__restrict__ cx, T *__restrict__ cy,
            T *__restrict__ cz, T *__restrict__ cmag, T inv_2h) {
-  int i, j, k;
-  if (!cell_of_thread(g, i, j, k)) return;
-  cell_curl(g, u, v, w, cx, cy, cz, cmag, inv_2h, i, j, k);
+  for_column_cells(g, [&](int i, int j, int k) {
+    cell_curl(g, u, v, w, cx, cy, cz, cmag, inv_2h, i, j, k);
+  });
 }
 
 // Pass 2: confinement force on 2..n-3 (:284-316), buoyancy lift on 1..n-2
@@ -213,11 +232,11 @@ __global__ void __launch_bounds__(kTx *kTy)
                    const T *__restrict__ cx, const T *__restrict__ cy,
                    const T *__restrict__ cz, const T *__restrict__ cmag, T dt, T eps_h,
                    T inv_2h, T beta, T alpha) {
-  int i, j, k;
-  if (!cell_of_thread(g, i, j, k)) return;
-  const int c = (k * g.ny + j) * g.nx + i;
-  cell_confine_buoy(g, u, v, w, rho[c], temp[c], cx, cy, cz, cmag, dt, eps_h, inv_2h, beta,
-                    alpha, i, j, k);
+  for_column_cells(g, [&](int i, int j, int k) {
+    const int c = (k * g.ny + j) * g.nx + i;
+    cell_confine_buoy(g, u, v, w, rho[c], temp[c], cx, cy, cz, cmag, dt, eps_h, inv_2h, beta,
+                      alpha, i, j, k);
+  });
 }
 
 // ---- compute_divergence_norm (src/fluid.rs:333-353) ------------------------
@@ -231,6 +250,7 @@ __global__ void __launch_bounds__(kBlock)
                  double *__restrict__ partials, double inv_h, double h) {
   __shared__ double scratch[kWarps * 2];
   double acc[2] = {0.0, 0.0};
+#pragma unroll 2
   for (int c = blockIdx.x * kBlock + threadIdx.x; c < g.n; c += gridDim.x * kBlock) {
     int i, j, k;
     decode(g, c, i, j, k);
@@ -283,9 +303,9 @@ template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
     k_project(Dims g, T *__restrict__ u, T *__restrict__ v, T *__restrict__ w,
               const double *__restrict__ p, double inv_h) {
-  int i, j, k;
-  if (!cell_of_thread(g, i, j, k)) return;
-  cell_project(g, u, v, w, p, inv_h, i, j, k);
+  for_column_cells(g, [&](int i, int j, int k) {
+    cell_project(g, u, v, w, p, inv_h, i, j, k);
+  });
 }
 
 // ---- sources -----------------------------------------------------------------
@@ -351,6 +371,7 @@ __global__ void __launch_bounds__(kBlock)
   (void)sx;
   (void)sy;
   (void)sz;
+#pragma unroll 2
   for (int c = blockIdx.x * kBlock + threadIdx.x; c < g.n; c += gridDim.x * kBlock) {
     int i, j, k;
     decode(g, c, i, j, k);
@@ -426,7 +447,7 @@ template <typename T>
 void launch_advect_fwd(const Dims &g, const T *u, const T *v, const T *w, const T *src,
                        T *fwd, double dt, cudaStream_t st) {
   const double scale = dt / g.h;
-  k_advect_fwd<T><<<plane_grid(g), dim3(kTx, kTy), 0, st>>>(g, u, v, w, src, fwd, T(scale));
+  k_advect_fwd<T><<<column_grid(g), dim3(kTx, kTy), 0, st>>>(g, u, v, w, src, fwd, T(scale));
 }
 
 template <typename T>
@@ -435,20 +456,20 @@ void launch_advect_mc(const Dims &g, const T *u, const T *v, const T *w, const T
                       cudaStream_t st) {
   const double scale_f = dt / g.h;
   const double scale_b = (-dt) / g.h;
-  k_advect_mc<T><<<plane_grid(g), dim3(kTx, kTy), 0, st>>>(
+  k_advect_mc<T><<<column_grid(g), dim3(kTx, kTy), 0, st>>>(
       g, u, v, w, src, fwd, out, T(scale_f), T(scale_b), T(dissipation), nonneg ? 1 : 0);
 }
 
 template <typename T>
 void launch_wall_bc(const Dims &g, T *u, T *v, T *w, cudaStream_t st) {
-  k_wall_bc<T><<<plane_grid(g), dim3(kTx, kTy), 0, st>>>(g, u, v, w);
+  k_wall_bc<T><<<column_grid(g), dim3(kTx, kTy), 0, st>>>(g, u, v, w);
 }
 
 template <typename T>
 void launch_curl(const Dims &g, const T *u, const T *v, const T *w, T *cx, T *cy, T *cz,
                  T *cmag, cudaStream_t st) {
   const double inv_2h = 0.5 / g.h;
-  k_curl<T><<<plane_grid(g), dim3(kTx, kTy), 0, st>>>(g, u, v, w, cx, cy, cz, cmag,
+  k_curl<T><<<column_grid(g), dim3(kTx, kTy), 0, st>>>(g, u, v, w, cx, cy, cz, cmag,
                                                       T(inv_2h));
 }
 
@@ -458,7 +479,7 @@ void launch_confine_buoy(const Dims &g, T *u, T *v, T *w, const T *rho, const T 
                          double eps, double beta, double alpha, cudaStream_t st) {
   const double inv_2h = 0.5 / g.h;
   const double eps_h = eps * g.h;
-  k_confine_buoy<T><<<plane_grid(g), dim3(kTx, kTy), 0, st>>>(
+  k_confine_buoy<T><<<column_grid(g), dim3(kTx, kTy), 0, st>>>(
       g, u, v, w, rho, temp, cx, cy, cz, cmag, T(dt), T(eps_h), T(inv_2h), T(beta),
       T(alpha));
 }
@@ -474,7 +495,7 @@ void launch_divergence(const Dims &g, const T *u, const T *v, const T *w, double
 
 template <typename T>
 void launch_project(const Dims &g, T *u, T *v, T *w, const double *p, cudaStream_t st) {
-  k_project<T><<<plane_grid(g), dim3(kTx, kTy), 0, st>>>(g, u, v, w, p, 1.0 / g.h);
+  k_project<T><<<column_grid(g), dim3(kTx, kTy), 0, st>>>(g, u, v, w, p, 1.0 / g.h);
 }
 
 template <typename T>

@@ -8,6 +8,7 @@ comparison therefore runs in two halves:
 
   python tests/large_accuracy.py oracle c2_cg OUTDIR   # CPU, writes OUTDIR/oracle_c2_cg.npz
   python tests/large_accuracy.py gpu c2_cg OUTDIR      # B200, reads that file
+  python tests/large_accuracy.py converged c2_cg OUTDIR  # B200 only, no oracle
 
 The oracle's final fields are stored as float32 (relative resolution ~6e-8,
 well below the 1e-5 / 1e-4 tolerances checked).  `gpu` runs each form of the
@@ -76,7 +77,37 @@ def run_gpu(name: str, out: str) -> int:
     return 0 if ok else 1
 
 
+def run_converged(name: str, iters: int = 5000) -> int:
+    """The mixed form against the FP64 form when every solve converges (CG to
+    the configuration's 1e-6 with an iteration cap high enough that it is
+    never reached): separates the precision of the mixed form from the
+    sensitivity of a solve truncated at 200 iterations."""
+    import aether_fluid as af
+    from helpers import max_abs, rel_l2
+    plume, _ = configs()[name]
+    if plume.solver != "cg":
+        print("converged mode applies to CG configurations")
+        return 2
+    got, its = {}, {}
+    for form in ("fp64", "mixed"):
+        s = plume.build(precision=af.Precision.FP64 if form == "fp64" else af.Precision.MIXED)
+        s.set_params(solver_iters=iters, mixed_inner_iters=iters)
+        _, infos = s.run(plume.steps, plume.dt, 0.0, plume.dt)
+        got[form] = {f: s.get_field(f) for f in FIELDS}
+        its[form] = {"mean_solver_iters": float(np.mean([i.iterations for i in infos])),
+                     "all_converged": bool(all(i.converged for i in infos))}
+        s.close()
+    row = {"config": name, "compare": "mixed vs fp64, converged solves", "iteration_cap": iters,
+           "rel_l2": {f: rel_l2(got["mixed"][f], got["fp64"][f]) for f in FIELDS},
+           "max_abs": {f: max_abs(got["mixed"][f], got["fp64"][f]) for f in FIELDS}, **its}
+    row["within_mixed_tolerance"] = all(v <= TOL["mixed"] for v in row["rel_l2"].values())
+    print(json.dumps(row), flush=True)
+    return 0
+
+
 def main() -> int:
+    if len(sys.argv) == 4 and sys.argv[1] == "converged" and sys.argv[2] in configs():
+        return run_converged(sys.argv[2])
     if len(sys.argv) != 4 or sys.argv[1] not in ("oracle", "gpu") or sys.argv[2] not in configs():
         print(__doc__)
         return 2
