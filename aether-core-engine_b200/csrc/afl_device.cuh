@@ -75,6 +75,51 @@ __device__ __forceinline__ Footprint<T> footprint(const Dims &g, T x, T y, T z) 
   return f;
 }
 
+// The footprint of the point (i, j, k) - (dx, dy, dz), a cell index moved by a
+// displacement.  In f64 this is footprint() of the moved position, the
+// reference's own expression (src/fluid.rs:160-162), bit for bit.
+template <typename T>
+__device__ __forceinline__ Footprint<T> footprint_at(const Dims &g, int i, int j, int k, T dx,
+                                                     T dy, T dz) {
+  return footprint(g, T(i) - dx, T(j) - dy, T(k) - dz);
+}
+
+// In f32 the moved position i - d, formed as one number near i, keeps only
+// ~1e-5 cell of the displacement at i ~ 100 (a relative error of 1e-3 in a
+// 0.005-cell step of the smoke).  Unclamped, the corner and weight follow from
+// the displacement alone: floor(i - d) = i + floor(-d) and the weight is
+// -d - floor(-d), both at the displacement's own precision.  The clamp test
+// still uses the moved position; near the clamp bounds the two agree to a few
+// ulps, which keeps the corner inside [0, n-2].
+__device__ __forceinline__ void axis_at(int i, int n, float d, int &i0, float &t) {
+  const float p = float(i) - d;
+  const float hi = float(n) - 1.500001f;
+  if (p < 0.5f) {
+    i0 = 0;
+    t = 0.5f;
+  } else if (p > hi) {
+    const float f = floorf(hi);
+    i0 = static_cast<int>(f);
+    t = hi - f;
+  } else {
+    const float f = floorf(-d);
+    i0 = i + static_cast<int>(f);
+    t = -d - f;
+  }
+}
+
+template <>
+__device__ __forceinline__ Footprint<float> footprint_at<float>(const Dims &g, int i, int j, int k,
+                                                                float dx, float dy, float dz) {
+  int i0, j0, k0;
+  Footprint<float> f;
+  axis_at(i, g.nx, dx, i0, f.tx);
+  axis_at(j, g.ny, dy, j0, f.ty);
+  axis_at(k, g.nz, dz, k0, f.tz);
+  f.base = (k0 * g.ny + j0) * g.nx + i0;
+  return f;
+}
+
 // sample_trilinear (src/fluid.rs:110-127): x-lerps, then y, then z, each as
 // a*(1-t) + b*t.
 template <typename T>

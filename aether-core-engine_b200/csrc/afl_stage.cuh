@@ -62,10 +62,7 @@ __device__ __forceinline__ void cell_advect_fwd(const Dims &g, const T *__restri
   const int c = (k * g.ny + j) * g.nx + i;
   T out = T(0);
   if (interior(g, i, j, k)) {
-    const T bx = T(i) - scale * u[c];
-    const T by = T(j) - scale * v[c];
-    const T bz = T(k) - scale * w[c];
-    out = trilinear(src, g, footprint(g, bx, by, bz));
+    out = trilinear(src, g, footprint_at(g, i, j, k, scale * u[c], scale * v[c], scale * w[c]));
   }
   fwd[c] = out;
 }
@@ -107,13 +104,12 @@ __device__ __forceinline__ void cell_advect_mc(const Dims &g, const T *__restric
       val = fc;
     } else {
       // bwd[c] = sample of fwd at the forward-traced point (scale_b = -dt/h)
-      const T fx = T(i) - scale_b * uc;
-      const T fy = T(j) - scale_b * vc;
-      const T fz = T(k) - scale_b * wc;
-      const T bwd = trilinear(fwd, g, footprint(g, fx, fy, fz));
+      const T bwd = trilinear(fwd, g, footprint_at(g, i, j, k, scale_b * uc, scale_b * vc,
+                                                    scale_b * wc));
       const T mc = fc + T(0.5) * (src[c] - bwd);
       T lo, hi;
-      minmax8(src, g, footprint(g, bx, by, bz).base, lo, hi);
+      minmax8(src, g, footprint_at(g, i, j, k, scale_f * uc, scale_f * vc, scale_f * wc).base,
+              lo, hi);
       val = rs_clamp(mc, lo, hi);
     }
     res = val * dissipation;

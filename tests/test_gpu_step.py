@@ -115,7 +115,11 @@ def test_config_64cube_fp64_parity(af, oracle):
 
 
 def test_config_64cube_mixed_parity(af, oracle):
-    """Same plume in the mixed form: within 1e-4 relative L2 of the f64 oracle."""
+    """Same plume in the mixed form: within the stated 1e-4 relative L2 of the
+    f64 oracle, and in fact within 2e-5.  The f32 advection forms its
+    interpolation weights from the displacement, not from a moved position
+    rounded near the cell index; without that the velocities drift to ~4e-4
+    over a few hundred steps."""
     from aether_fluid.plume import Plume
     p = Plume(64, 64, 64, 50, seed=0)
     o = oracle_for(p, oracle)
@@ -125,6 +129,7 @@ def test_config_64cube_mixed_parity(af, oracle):
     for f in ("u", "v", "w", "density", "temperature"):
         err = rel_l2(s.get_field(f), o.field(f))
         assert err <= 1e-4, (f, err)
+        assert err <= 2e-5, (f, err)
 
 
 def test_sor_plume_fp64_bit_exact_short(af, oracle):
