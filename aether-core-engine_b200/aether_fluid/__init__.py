@@ -5,6 +5,7 @@ the C ABI of include/aether_fluid.h); this package is the host-side mirror of
 the reference's `FluidSolver3D` / `FluidMedium` interface (src/fluid.rs).
 """
 from ._lib import AetherFluidError, LIB_PATH, load  # noqa: F401
+from .medium import DeviceMedium  # noqa: F401
 from .solver import (  # noqa: F401
     Aabb,
     FluidMedium,

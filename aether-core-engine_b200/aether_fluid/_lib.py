@@ -106,6 +106,11 @@ _i = ctypes.c_int
 _sz = ctypes.c_size_t
 _dp = ctypes.POINTER(ctypes.c_double)
 _st = ctypes.c_int
+class AflRay(ctypes.Structure):
+    _fields_ = [("origin", ctypes.c_double * 3), ("dir", ctypes.c_double * 3),
+                ("t_min", ctypes.c_double), ("t_end", ctypes.c_double)]
+
+
 SIGNATURES = [
     ("afl_last_error", ctypes.c_char_p, []),
     ("afl_abi_version", ctypes.c_int, []),
@@ -159,6 +164,13 @@ SIGNATURES = [
     ("afl_adjoint_stats", _st, [_vp, _dp]),
     ("afl_solve_cg_noalloc", _st, [_vp, _vp, _sz, _sz, _sz, _i, _d, _vp,
                                     ctypes.POINTER(AflSolveInfo)]),
+    ("afl_medium_create", _st, [_vp, _dp, _dp, _d, _d, ctypes.POINTER(_vp)]),
+    ("afl_medium_destroy", _st, [_vp]),
+    ("afl_medium_info", _st, [_vp, _dp]),
+    ("afl_medium_sample_density_temp", _st, [_vp, _dp, _sz, _dp, _dp]),
+    ("afl_medium_transmittance", _st, [_vp, _vp, _sz, ctypes.c_uint64, _dp]),
+    ("afl_medium_sample_interaction", _st, [_vp, _vp, _sz, ctypes.c_uint64,
+                                            ctypes.POINTER(ctypes.c_int32), _dp, _dp, _dp]),
     ("afl_synchronize", _st, [_vp]),
     ("afl_stream", _vp, [_vp]),
 ]

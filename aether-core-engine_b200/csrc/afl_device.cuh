@@ -120,6 +120,41 @@ __device__ __forceinline__ Footprint<float> footprint_at<float>(const Dims &g, i
   return f;
 }
 
+// Rng::from_seed / next_u64 / next_f64 (src/rng.rs:20-88): SplitMix64 of the
+// seed xor a constant fills the four Xoshiro256++ words; next_f64 keeps the top
+// 53 bits.  Integer work, identical on host and device.
+struct XoshiroRng {
+  unsigned long long s[4];
+  __host__ __device__ static unsigned long long rotl(unsigned long long x, int k) {
+    return (x << k) | (x >> (64 - k));
+  }
+  __host__ __device__ explicit XoshiroRng(unsigned long long seed) {
+    unsigned long long sm = seed ^ 0xA5A55A5AF0F00F0Full;
+    for (int a = 0; a < 4; ++a) {
+      sm += 0x9E3779B97F4A7C15ull;
+      unsigned long long z = sm;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      s[a] = z ^ (z >> 31);
+    }
+    if ((s[0] | s[1] | s[2] | s[3]) == 0) s[0] = 1;
+  }
+  __host__ __device__ unsigned long long next_u64() {
+    const unsigned long long out = rotl(s[0] + s[3], 23) + s[0];
+    const unsigned long long t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = rotl(s[3], 45);
+    return out;
+  }
+  __host__ __device__ double next_f64() {
+    return static_cast<double>(next_u64() >> 11) * (1.0 / 9007199254740992.0);
+  }
+};
+
 // sample_trilinear (src/fluid.rs:110-127): x-lerps, then y, then z, each as
 // a*(1-t) + b*t.
 template <typename T>

@@ -11,6 +11,8 @@
 
 #include "afl_device.cuh"
 
+struct afl_solver;  // include/aether_fluid.h
+
 namespace afl {
 
 // Device-resident per-step report written by the Poisson kernels (mirrors
@@ -231,5 +233,18 @@ int persistent_blocks_cg_f64();
 int persistent_blocks_sor_f64();
 int persistent_blocks_cg_mixed();
 int persistent_blocks_sor_mixed();
+
+// Read-only view of a solver's device state for other units of the library
+// (afl_medium.cu): the grid, the device, the stream and the density and
+// temperature fields (f64 or f32 by precision).
+struct SolverView {
+  Dims g;
+  int device;
+  cudaStream_t stream;
+  bool f64;
+  const void *density;
+  const void *temperature;
+};
+bool solver_view(const afl_solver *s, SolverView *out);
 
 }  // namespace afl

@@ -532,6 +532,19 @@ void set_last_error_text(const char *msg) { g_last_error = msg ? msg : ""; }
 }  // namespace afl
 
 // ============================================================================
+namespace afl {
+bool solver_view(const afl_solver *s, SolverView *out) {
+  if (!s || !out) return false;
+  out->g = s->g;
+  out->device = s->device;
+  out->stream = s->stream;
+  out->f64 = s->precision == AFL_PRECISION_FP64;
+  out->density = s->fld[3];
+  out->temperature = s->fld[4];
+  return true;
+}
+}  // namespace afl
+
 extern "C" {
 
 const char *afl_last_error(void) { return g_last_error.c_str(); }

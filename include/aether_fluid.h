@@ -318,6 +318,49 @@ afl_status afl_adjoint_backward(afl_adjoint *a, const double *rho_bar, double *u
  * iterations, adjoint CG iterations} */
 afl_status afl_adjoint_stats(const afl_adjoint *a, double out[4]);
 
+/* ---- FluidMedium on the device (src/fluid.rs:687-874) ----------------------
+ * The renderer's medium queries over a snapshot of a solver's density and
+ * temperature, kept on the GPU.  afl_medium_create replaces
+ * FluidMedium::from_solver (src/fluid.rs:703-732): it copies the two fields
+ * (as f64), takes the max density and the majorant
+ * max(max_density * sigma_t_scale, 1e-4), clamps phase_g to [-0.9, 0.9] and
+ * orders the bounds as Aabb::new does.  Later steps of the solver do not change
+ * the medium.
+ *
+ * Queries take host arrays and return host arrays; the medium keeps device
+ * staging buffers that grow to the largest batch seen.  A ray is given as in
+ * Ray::new (the direction is normalised inside, src/math.rs:763-774) plus the
+ * end of its segment: `surface_t` of sample_interaction (src/fluid.rs:793-799) or
+ * `max_dist` of transmittance (src/fluid.rs:841).  Each ray draws from its own
+ * Rng::from_seed(seed + ray index) stream, so results do not depend on batch
+ * order or size (the reference threads one generator through a path). */
+typedef struct afl_medium afl_medium;
+typedef struct afl_ray {
+  double origin[3];
+  double dir[3];
+  double t_min; /* Ray::t_min */
+  double t_end; /* surface_t (interaction) or max_dist (transmittance) */
+} afl_ray;
+afl_status afl_medium_create(afl_solver *s, const double bounds_min[3],
+                             const double bounds_max[3], double sigma_t_scale, double phase_g,
+                             afl_medium **out);
+afl_status afl_medium_destroy(afl_medium *m);
+/* out = {max_density, majorant_sigma_t, phase_g, sigma_t_scale} */
+afl_status afl_medium_info(const afl_medium *m, double out[4]);
+/* sample_density_and_temp (src/fluid.rs:739-786) at n points (x, y, z). */
+afl_status afl_medium_sample_density_temp(afl_medium *m, const double *points, size_t n,
+                                          double *density, double *temperature);
+/* Ratio-tracking transmittance in [0, 1] (src/fluid.rs:840-874) per ray. */
+afl_status afl_medium_transmittance(afl_medium *m, const afl_ray *rays, size_t n,
+                                    uint64_t seed, double *transmittance);
+/* Delta-tracking free flight (src/fluid.rs:792-838) per ray: hit[r] = 1 and the
+ * distance t, density and temperature at ray.at(t) when the ray interacts
+ * before t_end, else hit[r] = 0 (t, density, temperature = 0).  Any of t,
+ * density, temperature may be NULL. */
+afl_status afl_medium_sample_interaction(afl_medium *m, const afl_ray *rays, size_t n,
+                                         uint64_t seed, int32_t *hit, double *t,
+                                         double *density, double *temperature);
+
 /* ---- a pressure solve that allocates nothing --------------------------------
  * No counterpart in the reference.  For callers that may not allocate device
  * memory -- code recorded into a CUDA graph, real-time/render threads that

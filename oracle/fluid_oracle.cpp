@@ -680,3 +680,220 @@ void ofl_rng_f64(uint64_t seed, size_t n, double *out) {
 }
 
 }  // extern "C"
+
+// ---- FluidMedium (src/fluid.rs:687-874) --------------------------------------
+namespace {
+
+struct Medium {
+  const double *dens, *temp;
+  size_t nx, ny, nz;
+  double bmin[3], bmax[3];
+  double sigma_t_scale, majorant, max_density;
+  size_t idx(size_t i, size_t j, size_t k) const { return (k * ny + j) * nx + i; }
+};
+
+Medium make_medium(const double *dens, const double *temp, size_t nx, size_t ny, size_t nz,
+                   const double *bmin, const double *bmax, double sigma_t_scale) {
+  Medium m{dens, temp, nx, ny, nz, {}, {}, sigma_t_scale, 0.0, 0.0};
+  for (int a = 0; a < 3; ++a) {  // Aabb::new (src/math.rs:794-799): min_elem / max_elem
+    m.bmin[a] = std::fmin(bmin[a], bmax[a]);
+    m.bmax[a] = std::fmax(bmin[a], bmax[a]);
+  }
+  // FluidMedium::from_solver (src/fluid.rs:703-708)
+  double mx = 0.0;
+  for (size_t c = 0; c < nx * ny * nz; ++c) mx = std::fmax(mx, dens[c]);
+  m.max_density = mx;
+  m.majorant = std::fmax(mx * sigma_t_scale, 1e-4);
+  return m;
+}
+
+// sample_density_and_temp (src/fluid.rs:739-786)
+void med_sample(const Medium &m, const double p[3], double &rho, double &tmp) {
+  if (p[0] < m.bmin[0] || p[0] > m.bmax[0] || p[1] < m.bmin[1] || p[1] > m.bmax[1] ||
+      p[2] < m.bmin[2] || p[2] > m.bmax[2]) {
+    rho = 0.0;
+    tmp = 0.0;
+    return;
+  }
+  double ext[3], uvw[3];
+  for (int a = 0; a < 3; ++a) {
+    ext[a] = std::fmax(m.bmax[a] - m.bmin[a], 0.0);  // Aabb::extent (src/math.rs:832-834)
+    uvw[a] = (p[a] - m.bmin[a]) / std::fmax(ext[a], 1e-9);
+  }
+  const double ux = uvw[0], uy = uvw[1], uz = uvw[2];
+  const double fx = rs_clamp(4.0 * ux * (1.0 - ux), 0.0, 1.0);
+  const double fz = rs_clamp(4.0 * uz * (1.0 - uz), 0.0, 1.0);
+  const double fy = rs_clamp(1.0 - (std::fmax(uy - 0.95, 0.0) / 0.05), 0.0, 1.0);
+  const double feather = std::sqrt(fx * fz * fy);
+  const double gx = rs_clamp(ux * static_cast<double>(m.nx - 1), 0.5,
+                             static_cast<double>(m.nx) - 1.500001);
+  const double gy = rs_clamp(uy * static_cast<double>(m.ny - 1), 0.5,
+                             static_cast<double>(m.ny) - 1.500001);
+  const double gz = rs_clamp(uz * static_cast<double>(m.nz - 1), 0.5,
+                             static_cast<double>(m.nz) - 1.500001);
+  const size_t i0 = rs_as_usize(std::floor(gx));
+  const size_t j0 = rs_as_usize(std::floor(gy));
+  const size_t k0 = rs_as_usize(std::floor(gz));
+  const double tx = gx - static_cast<double>(i0);
+  const double ty = gy - static_cast<double>(j0);
+  const double tz = gz - static_cast<double>(k0);
+  auto trilin = [&](const double *buf) {
+    const double c000 = buf[m.idx(i0, j0, k0)];
+    const double c100 = buf[m.idx(i0 + 1, j0, k0)];
+    const double c010 = buf[m.idx(i0, j0 + 1, k0)];
+    const double c110 = buf[m.idx(i0 + 1, j0 + 1, k0)];
+    const double c001 = buf[m.idx(i0, j0, k0 + 1)];
+    const double c101 = buf[m.idx(i0 + 1, j0, k0 + 1)];
+    const double c011 = buf[m.idx(i0, j0 + 1, k0 + 1)];
+    const double c111 = buf[m.idx(i0 + 1, j0 + 1, k0 + 1)];
+    const double c00 = c000 * (1.0 - tx) + c100 * tx;
+    const double c10 = c010 * (1.0 - tx) + c110 * tx;
+    const double c01 = c001 * (1.0 - tx) + c101 * tx;
+    const double c11 = c011 * (1.0 - tx) + c111 * tx;
+    return (c00 * (1.0 - ty) + c10 * ty) * (1.0 - tz) + (c01 * (1.0 - ty) + c11 * ty) * tz;
+  };
+  rho = trilin(m.dens) * feather;
+  tmp = trilin(m.temp) * feather;
+}
+
+// Ray::new (src/math.rs:763-774) with Vec3::normalize (src/math.rs:58-65); the
+// length is dot(self, self).sqrt() with dot written as mul_add
+// (src/math.rs:34-36).
+struct Ray {
+  double o[3], d[3], inv[3];
+  double t_min, t_end;
+  void at(double t, double p[3]) const {
+    for (int a = 0; a < 3; ++a) p[a] = o[a] + d[a] * t;  // Ray::at (src/math.rs:776-779)
+  }
+};
+
+Ray make_ray(const double *r8) {
+  Ray r;
+  for (int a = 0; a < 3; ++a) r.o[a] = r8[a];
+  const double x = r8[3], y = r8[4], z = r8[5];
+  const double len = std::sqrt(std::fma(x, x, std::fma(y, y, z * z)));
+  if (len > 1e-18) {
+    const double s = 1.0 / len;
+    r.d[0] = x * s;
+    r.d[1] = y * s;
+    r.d[2] = z * s;
+  } else {
+    r.d[0] = 0.0;
+    r.d[1] = 0.0;
+    r.d[2] = 1.0;
+  }
+  for (int a = 0; a < 3; ++a) r.inv[a] = 1.0 / r.d[a];
+  r.t_min = r8[6];
+  r.t_end = r8[7];
+  return r;
+}
+
+// Aabb::intersect (src/math.rs:859-890)
+bool intersect(const Medium &m, const Ray &r, double t_min, double t_max, double &t0,
+               double &t1) {
+  for (int a = 0; a < 3; ++a) {
+    const double ta = (m.bmin[a] - r.o[a]) * r.inv[a];
+    const double tb = (m.bmax[a] - r.o[a]) * r.inv[a];
+    t_min = std::fmax(t_min, std::fmin(ta, tb));
+    t_max = std::fmin(t_max, std::fmax(ta, tb));
+    if (a < 2 && t_max < t_min) return false;
+  }
+  if (!(t_max >= t_min)) return false;
+  t0 = t_min;
+  t1 = t_max;
+  return true;
+}
+
+// transmittance (src/fluid.rs:840-874)
+double transmittance(const Medium &m, const Ray &r, Xoshiro &rng) {
+  if (m.max_density <= 1e-6) return 1.0;
+  double t_enter, t_exit;
+  if (!intersect(m, r, r.t_min, r.t_end, t_enter, t_exit)) return 1.0;
+  double t = std::fmax(t_enter, r.t_min);
+  const double limit = std::fmin(t_exit, r.t_end);
+  if (t >= limit) return 1.0;
+  double tr = 1.0;
+  const double inv_maj = 1.0 / m.majorant;
+  for (int s = 0; s < 256; ++s) {
+    const double u = std::fmax(1.0 - rng.next_f64(), 1e-15);
+    t -= std::log(u) * inv_maj;
+    if (t >= limit) break;
+    double p[3], rho, tmp;
+    r.at(t, p);
+    med_sample(m, p, rho, tmp);
+    const double sigma_t = std::fmin(rho * m.sigma_t_scale, m.majorant);
+    tr *= 1.0 - sigma_t * inv_maj;
+    if (tr < 0.05) {
+      const double q = std::fmin(1.0 - tr, 0.95);
+      if (rng.next_f64() < q) return 0.0;
+      tr /= 1.0 - q;
+    }
+  }
+  return rs_clamp(tr, 0.0, 1.0);
+}
+
+// sample_interaction (src/fluid.rs:792-838)
+bool interaction(const Medium &m, const Ray &r, Xoshiro &rng, double &t_hit, double &rho_hit,
+                 double &tmp_hit) {
+  if (m.max_density <= 1e-6) return false;
+  double t_enter, t_exit;
+  if (!intersect(m, r, r.t_min, r.t_end, t_enter, t_exit)) return false;
+  double t = std::fmax(t_enter, r.t_min);
+  const double limit = std::fmin(t_exit, r.t_end);
+  if (t >= limit) return false;
+  const double inv_maj = 1.0 / m.majorant;
+  for (int s = 0; s < 256; ++s) {
+    const double u = std::fmax(1.0 - rng.next_f64(), 1e-15);
+    t -= std::log(u) * inv_maj;
+    if (t >= limit) return false;
+    double p[3], rho, tmp;
+    r.at(t, p);
+    med_sample(m, p, rho, tmp);
+    const double sigma_t = rho * m.sigma_t_scale;
+    if (rng.next_f64() * m.majorant < sigma_t) {
+      t_hit = t;
+      rho_hit = rho;
+      tmp_hit = tmp;
+      return true;
+    }
+  }
+  return false;
+}
+
+}  // namespace
+
+extern "C" {
+
+void ofl_medium_sample(const double *dens, const double *temp, size_t nx, size_t ny, size_t nz,
+                       const double *bmin, const double *bmax, const double *pts, size_t n,
+                       double *rho, double *tmp) {
+  const Medium m = make_medium(dens, temp, nx, ny, nz, bmin, bmax, 1.0);
+  for (size_t c = 0; c < n; ++c) med_sample(m, pts + 3 * c, rho[c], tmp[c]);
+}
+
+void ofl_medium_transmittance(const double *dens, const double *temp, size_t nx, size_t ny,
+                              size_t nz, const double *bmin, const double *bmax,
+                              double sigma_t_scale, const double *rays, size_t n, uint64_t seed,
+                              double *tr) {
+  const Medium m = make_medium(dens, temp, nx, ny, nz, bmin, bmax, sigma_t_scale);
+  for (size_t c = 0; c < n; ++c) {
+    Xoshiro rng(seed + static_cast<uint64_t>(c));
+    tr[c] = transmittance(m, make_ray(rays + 8 * c), rng);
+  }
+}
+
+void ofl_medium_interaction(const double *dens, const double *temp, size_t nx, size_t ny,
+                            size_t nz, const double *bmin, const double *bmax,
+                            double sigma_t_scale, const double *rays, size_t n, uint64_t seed,
+                            int32_t *hit, double *t, double *rho, double *tmp) {
+  const Medium m = make_medium(dens, temp, nx, ny, nz, bmin, bmax, sigma_t_scale);
+  for (size_t c = 0; c < n; ++c) {
+    Xoshiro rng(seed + static_cast<uint64_t>(c));
+    double th = 0.0, rh = 0.0, qh = 0.0;
+    hit[c] = interaction(m, make_ray(rays + 8 * c), rng, th, rh, qh) ? 1 : 0;
+    t[c] = th;
+    rho[c] = rh;
+    tmp[c] = qh;
+  }
+}
+}  // extern "C"

@@ -2,7 +2,8 @@
  * fluid_oracle.h -- CPU restatement of the reference smoke solver.
  *
  * TEST INFRASTRUCTURE ONLY.  This is the oracle: a scalar, single-threaded,
- * f64 restatement of `FluidSolver3D` (src/fluid.rs:23-673) and of the
+ * f64 restatement of `FluidSolver3D` (src/fluid.rs:23-673), of the volume
+ * queries of `FluidMedium` (src/fluid.rs:687-874) and of the
  * SplitMix64/Xoshiro256++ generator (src/rng.rs:5-88) of
  * vanovri/aether-core-engine.  Only tests/, __graft_entry__.smoke() and the
  * CPU-baseline leg of bench.py may load it, and only as the checker.  The
@@ -105,6 +106,23 @@ void ofl_init_velocity_noise(ofl_solver *s, uint64_t seed, double lo,
 /* Generator access for tests (src/rng.rs:21-88). */
 void ofl_rng_u64(uint64_t seed, size_t n, uint64_t *out);
 void ofl_rng_f64(uint64_t seed, size_t n, double *out);
+
+/* FluidMedium volume queries (src/fluid.rs:687-874) over host arrays of
+ * nx*ny*nz doubles.  Bounds are ordered as Aabb::new does; the max density
+ * and the majorant are taken as FluidMedium::from_solver does.  A ray is 8
+ * doubles: origin[3], dir[3] (normalised as Ray::new does), t_min, t_end.
+ * Ray r draws from Rng::from_seed(seed + r). */
+void ofl_medium_sample(const double *dens, const double *temp, size_t nx, size_t ny, size_t nz,
+                       const double *bmin, const double *bmax, const double *pts, size_t n,
+                       double *rho, double *tmp);
+void ofl_medium_transmittance(const double *dens, const double *temp, size_t nx, size_t ny,
+                              size_t nz, const double *bmin, const double *bmax,
+                              double sigma_t_scale, const double *rays, size_t n, uint64_t seed,
+                              double *tr);
+void ofl_medium_interaction(const double *dens, const double *temp, size_t nx, size_t ny,
+                            size_t nz, const double *bmin, const double *bmax,
+                            double sigma_t_scale, const double *rays, size_t n, uint64_t seed,
+                            int32_t *hit, double *t, double *rho, double *tmp);
 
 #ifdef __cplusplus
 }

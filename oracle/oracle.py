@@ -85,6 +85,15 @@ def lib():
         L.ofl_init_velocity_noise.argtypes = [vp, ctypes.c_uint64, d, d]
         L.ofl_rng_u64.argtypes = [ctypes.c_uint64, sz, ctypes.POINTER(ctypes.c_uint64)]
         L.ofl_rng_f64.argtypes = [ctypes.c_uint64, sz, _c_double_p]
+        L.ofl_medium_sample.argtypes = [_c_double_p, _c_double_p, sz, sz, sz, _c_double_p,
+                                        _c_double_p, _c_double_p, sz, _c_double_p, _c_double_p]
+        L.ofl_medium_transmittance.argtypes = [_c_double_p, _c_double_p, sz, sz, sz, _c_double_p,
+                                               _c_double_p, d, _c_double_p, sz, ctypes.c_uint64,
+                                               _c_double_p]
+        L.ofl_medium_interaction.argtypes = [_c_double_p, _c_double_p, sz, sz, sz, _c_double_p,
+                                             _c_double_p, d, _c_double_p, sz, ctypes.c_uint64,
+                                             ctypes.POINTER(ctypes.c_int32), _c_double_p,
+                                             _c_double_p, _c_double_p]
         _lib = L
     return _lib
 
@@ -212,3 +221,42 @@ def rng_f64(seed: int, n: int) -> np.ndarray:
     out = np.zeros(n)
     lib().ofl_rng_f64(seed, n, _dptr(out))
     return out
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def medium_sample(dens, temp, shape, bmin, bmax, points):
+    """FluidMedium::sample_density_and_temp (src/fluid.rs:739-786) at points [n, 3]."""
+    dens, temp, pts = _f64(dens).ravel(), _f64(temp).ravel(), _f64(points).reshape(-1, 3)
+    n = pts.shape[0]
+    rho, tmp = np.zeros(n), np.zeros(n)
+    lib().ofl_medium_sample(_dptr(dens), _dptr(temp), *shape, _dptr(_f64(bmin)),
+                            _dptr(_f64(bmax)), _dptr(pts), n, _dptr(rho), _dptr(tmp))
+    return rho, tmp
+
+
+def medium_transmittance(dens, temp, shape, bmin, bmax, sigma_t_scale, rays, seed):
+    """FluidMedium::transmittance (src/fluid.rs:840-874) per ray; rays [n, 8] =
+    origin, dir, t_min, t_end; ray r uses Rng::from_seed(seed + r)."""
+    dens, temp, r = _f64(dens).ravel(), _f64(temp).ravel(), _f64(rays).reshape(-1, 8)
+    n = r.shape[0]
+    tr = np.zeros(n)
+    lib().ofl_medium_transmittance(_dptr(dens), _dptr(temp), *shape, _dptr(_f64(bmin)),
+                                   _dptr(_f64(bmax)), sigma_t_scale, _dptr(r), n, seed, _dptr(tr))
+    return tr
+
+
+def medium_interaction(dens, temp, shape, bmin, bmax, sigma_t_scale, rays, seed):
+    """FluidMedium::sample_interaction (src/fluid.rs:792-838) per ray: (hit, t,
+    density, temperature)."""
+    dens, temp, r = _f64(dens).ravel(), _f64(temp).ravel(), _f64(rays).reshape(-1, 8)
+    n = r.shape[0]
+    hit = np.zeros(n, dtype=np.int32)
+    t, rho, tmp = np.zeros(n), np.zeros(n), np.zeros(n)
+    lib().ofl_medium_interaction(_dptr(dens), _dptr(temp), *shape, _dptr(_f64(bmin)),
+                                 _dptr(_f64(bmax)), sigma_t_scale, _dptr(r), n, seed,
+                                 hit.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _dptr(t),
+                                 _dptr(rho), _dptr(tmp))
+    return hit, t, rho, tmp
