@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--ensemble-steps", type=int, default=100)
     ap.add_argument("--no-large", action="store_true",
                     help="skip the 256^3 x 100-step mixed/FP64 measurement")
+    ap.add_argument("--no-medium", action="store_true",
+                    help="skip the device medium-query measurement")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the reverse-mode (adjoint) measurement")
     ap.add_argument("--adjoint-directions", type=int, default=16,
@@ -452,6 +454,54 @@ def time_adjoint(ndir: int, torch, n: int = 96, steps: int = 64, every: int = 8)
             "gradient_norm": gnorm, "fd_directions": ndir, "fd": fd}
 
 
+def time_medium(torch, n_rays: int = 1 << 20, cpu_rays: int = 4000) -> dict:
+    """The renderer's medium queries (FluidMedium::transmittance and
+    ::sample_interaction, src/fluid.rs:792-874) on the device: a 128^3 plume
+    after 100 FP64 steps, the medium bounds and scales of the reference scene
+    (src/main.rs:109: Aabb (-2.25, 0.22, -2.15)-(2.25, 5.15, 1.45), sigma_t
+    scale 1.42, g 0.34), 2^20 rays from a camera-like origin towards uniform
+    points of the box.  Rays/s through the public API with host buffers
+    (copies included), next to the CPU oracle on a bounded sample of the same
+    rays (1 core)."""
+    import numpy as np
+    import aether_fluid as af
+    from aether_fluid.plume import Plume
+    p = Plume(128, 128, 128, 100, seed=0)
+    s = p.build()
+    s.run(p.steps, p.dt, 0.0, p.dt)
+    lo, hi = (-2.25, 0.22, -2.15), (2.25, 5.15, 1.45)
+    m = af.DeviceMedium.from_solver(s, af.Aabb(lo, hi), 1.42, 0.34)
+    rng = np.random.default_rng(0)
+    o = np.tile([0.0, 2.4, 9.0], (n_rays, 1))
+    target = rng.uniform(lo, hi, size=(n_rays, 3))
+    rays = np.column_stack([o, target - o, np.full(n_rays, 1e-4), np.full(n_rays, 20.0)])
+    m.transmittance(rays[:4096], 1)          # warm-up
+    m.sample_interaction(rays[:4096], 1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tr = m.transmittance(rays, 7)
+    t_tr = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    hit = m.sample_interaction(rays, 8)[0]
+    t_int = time.perf_counter() - t0
+    out = {"rays": n_rays, "grid": [128, 128, 128], "steps": p.steps,
+           "transmittance_rays_per_s": n_rays / t_tr, "interaction_rays_per_s": n_rays / t_int,
+           "mean_transmittance": float(tr.mean()), "interaction_fraction": float(hit.mean()),
+           "h2d_bytes": int(rays.nbytes), "unit": "rays/s (host buffers, copies included)"}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    d, q = s.get_field("density"), s.get_field("temperature")
+    t0 = time.perf_counter()
+    O.medium_transmittance(d, q, (128, 128, 128), lo, hi, 1.42, rays[:cpu_rays], 7)
+    t_cpu = time.perf_counter() - t0
+    out["cpu_oracle_transmittance_rays_per_s"] = cpu_rays / t_cpu
+    out["cpu_sample"] = f"first {cpu_rays} rays, 1 core"
+    m.close()
+    s.close()
+    return out
+
+
 def cpu_sample(n: int, seconds: float):
     """The oracle (f64, 1 thread) on the first steps of the same plume until
     `seconds` of CPU time have been spent."""
@@ -547,6 +597,13 @@ def run_ours(args):
         except Exception as exc:  # reported, never hides the headline
             large = {"error": str(exc)}
 
+    medium = None
+    if not args.no_medium and rank == 0:
+        try:
+            medium = time_medium(torch)
+        except Exception as exc:  # reported, never hides the headline
+            medium = {"error": str(exc)}
+
     adjoint = None
     if not args.no_adjoint:
         try:
@@ -629,6 +686,7 @@ def run_ours(args):
                          "peak_source": peak_kind},
             "variants": variants,
             "large_256": large,
+            "medium": medium,
             "ensemble": ensemble,
             "adjoint_fwd_ratio": adjoint.get("adjoint_fwd_ratio") if adjoint else None,
             "adjoint": adjoint,
