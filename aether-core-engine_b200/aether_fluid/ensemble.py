@@ -144,6 +144,12 @@ class Ensemble:
         check(self._lib.afl_ensemble_info(self._h, out))
         ctas = (ctypes.c_int32 * self.count)()
         check(self._lib.afl_ensemble_instance_ctas(self._h, ctas, self.count))
+        kz = ctypes.c_int32()
+        check(self._lib.afl_ensemble_tile_depth(self._h, ctypes.byref(kz)))
         return {"instances": out[0], "graph": bool(out[1]), "solver_ctas": out[2],
                 "cta_budget": out[3], "vector_width": out[4], "autotune_choice": out[5],
-                "instance_ctas": list(ctas)}
+                "instance_ctas": list(ctas), "tile_depth": kz.value}
+
+    def set_tile_depth(self, kz: int):
+        """z planes per CTA tile of the batched stage kernels (1, 2 or 4)."""
+        check(self._lib.afl_ensemble_set_tile_depth(self._h, kz))

@@ -110,6 +110,7 @@ struct afl_ensemble {
   void *d_inst = nullptr;  // EnsInstance<T>[count]
   int *d_blk_inst = nullptr;
   int blocks = 0;
+  int kz = 1;              // z planes per stage block (tile depth)
   double *d_tel_partials = nullptr;
   int *d_step = nullptr;
   double *d_tel_out = nullptr;
@@ -147,6 +148,11 @@ afl_status ens_alloc_as(afl_ensemble *e, P **out, size_t bytes) {
   ENS_TRY(ens_alloc(e, &v, bytes));
   *out = static_cast<P *>(v);
   return AFL_OK;
+}
+
+// Stage blocks of one instance: 32 x 8 tiles of kz z planes.
+int tile_blocks(const afl::Dims &g, int kz) {
+  return ((g.nx + 31) / 32) * ((g.ny + 7) / 8) * ((g.nz + kz - 1) / kz);
 }
 
 template <typename T>
@@ -190,15 +196,44 @@ afl_status build_descriptors(afl_ensemble *e, std::vector<int> &blk_inst) {
     d.src_r2 = r * r;
     d.src_rho = in.sphere_density;
     d.src_temp = in.sphere_temperature;
-    const int gx = (g.nx + 31) / 32, gy = (g.ny + 7) / 8;
+    d.kz = e->kz;
     d.blk_begin = static_cast<int>(blk_inst.size());
-    d.blk_count = gx * gy * g.nz;
+    d.blk_count = tile_blocks(g, e->kz);
     blk_inst.insert(blk_inst.end(), static_cast<size_t>(d.blk_count), m);
   }
   ENS_CUDA(cudaMemcpyAsync(e->d_inst, h.data(), sizeof(afl::EnsInstance<T>) * e->count,
                            cudaMemcpyHostToDevice, e->stream));
   ENS_CUDA(cudaStreamSynchronize(e->stream));
   return AFL_OK;
+}
+
+// Changes the tile depth of the stage kernels in place: the descriptors on the
+// device keep their current field pointers (the ping-pong state); only the
+// block ranges change, and the block table is rewritten.
+template <typename T>
+afl_status set_tile_depth_t(afl_ensemble *e, int kz) {
+  std::vector<afl::EnsInstance<T>> h(e->count);
+  ENS_CUDA(cudaStreamSynchronize(e->stream));
+  ENS_CUDA(cudaMemcpy(h.data(), e->d_inst, sizeof(afl::EnsInstance<T>) * e->count,
+                      cudaMemcpyDeviceToHost));
+  std::vector<int> blk_inst;
+  for (int m = 0; m < e->count; ++m) {
+    h[m].kz = kz;
+    h[m].blk_begin = static_cast<int>(blk_inst.size());
+    h[m].blk_count = tile_blocks(e->dims[m], kz);
+    blk_inst.insert(blk_inst.end(), static_cast<size_t>(h[m].blk_count), m);
+  }
+  ENS_CUDA(cudaMemcpy(e->d_inst, h.data(), sizeof(afl::EnsInstance<T>) * e->count,
+                      cudaMemcpyHostToDevice));
+  ENS_CUDA(cudaMemcpy(e->d_blk_inst, blk_inst.data(), sizeof(int) * blk_inst.size(),
+                      cudaMemcpyHostToDevice));
+  e->blocks = static_cast<int>(blk_inst.size());
+  e->kz = kz;
+  return AFL_OK;
+}
+
+afl_status set_tile_depth(afl_ensemble *e, int kz) {
+  return e->f64 ? set_tile_depth_t<double>(e, kz) : set_tile_depth_t<float>(e, kz);
 }
 
 // CTA split of the batched solve: proportional to the weights, at least one
@@ -587,13 +622,16 @@ afl_status afl_ensemble_download_field(afl_ensemble *e, int instance, int field,
   return AFL_OK;
 }
 
-// Times candidate CTA splits of the batched solve -- proportional to cells,
-// proportional to cells x observed iterations, and the cell split on 3/4 of
-// the co-resident CTAs -- one step each (after one untimed step), on a
-// snapshot of the state that is restored afterwards; keeps the fastest.
+// Times candidate layouts, one step each (after one untimed step), on a
+// snapshot of the state that is restored before every candidate and at the
+// end; keeps the fastest.  Candidates: CTA splits of the batched solve --
+// proportional to cells, proportional to cells x observed iterations, and the
+// cell split on 3/4 of the co-resident CTAs -- and then, with the best split,
+// stage tiles of 2 and 4 z planes besides 1.
 afl_status afl_ensemble_autotune(afl_ensemble *e, int32_t *choice) {
   if (!e) return fail(AFL_ERR_INVALID_ARGUMENT, "null ensemble");
   ENS_CUDA(cudaStreamSynchronize(e->stream));
+  const int kz0 = e->kz;
   const size_t desc_bytes = (e->f64 ? sizeof(afl::EnsInstance<double>)
                                     : sizeof(afl::EnsInstance<float>)) * e->count;
   std::vector<char> desc(desc_bytes);
@@ -609,7 +647,7 @@ afl_status afl_ensemble_autotune(afl_ensemble *e, int32_t *choice) {
       void *dst = nullptr;
       const cudaError_t err = cudaMalloc(&dst, bytes);
       if (err != cudaSuccess) {
-        for (void *s : snap) cudaFree(s);
+        for (void *sp : snap) cudaFree(sp);
         return cuda_fail(err, "autotune snapshot");
       }
       cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToDevice);
@@ -617,9 +655,10 @@ afl_status afl_ensemble_autotune(afl_ensemble *e, int32_t *choice) {
       live.push_back({src, bytes});
     }
   }
+  // the state and the descriptors as they were (tile depth kz0)
   auto restore = [&]() {
-    for (size_t s = 0; s < snap.size(); ++s)
-      cudaMemcpy(live[s].first, snap[s], live[s].second, cudaMemcpyDeviceToDevice);
+    for (size_t k = 0; k < snap.size(); ++k)
+      cudaMemcpy(live[k].first, snap[k], live[k].second, cudaMemcpyDeviceToDevice);
     cudaMemcpy(e->d_inst, desc.data(), desc_bytes, cudaMemcpyHostToDevice);
     cudaMemset(e->d_step, 0, sizeof(int));
   };
@@ -630,25 +669,28 @@ afl_status afl_ensemble_autotune(afl_ensemble *e, int32_t *choice) {
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
+  // one timed step of (split, tile depth); restores the state first
+  auto time_one = [&](const std::vector<int> &split, int kz, float *ms) -> afl_status {
+    ENS_TRY(build_systems(e, split));
+    restore();
+    ENS_TRY(set_tile_depth(e, kz));
+    ENS_TRY(enqueue(e));  // untimed
+    cudaEventRecord(t0, e->stream);
+    ENS_TRY(enqueue(e));
+    cudaEventRecord(t1, e->stream);
+    ENS_TRY(sync_status(e));
+    cudaEventElapsedTime(ms, t0, t1);
+    return AFL_OK;
+  };
   float best_ms = 1e30f;
-  int best = 0;
+  int best = 0, best_kz = kz0;
   afl_status st = AFL_OK;
   for (size_t c = 0; c < 3 && st == AFL_OK; ++c) {
     if (c == 1) cands.push_back(split_ctas(work, e->budget));
     if (c == 2) cands.push_back(split_ctas(cells, std::max(e->count, (3 * e->budget) / 4)));
-    st = build_systems(e, cands[c]);
-    if (st != AFL_OK) break;
-    restore();
-    st = enqueue(e);  // untimed
-    if (st != AFL_OK) break;
-    cudaEventRecord(t0, e->stream);
-    st = enqueue(e);
-    cudaEventRecord(t1, e->stream);
-    if (st != AFL_OK) break;
-    st = sync_status(e);
-    if (st != AFL_OK) break;
     float ms = 0.0f;
-    cudaEventElapsedTime(&ms, t0, t1);
+    st = time_one(cands[c], 1, &ms);
+    if (st != AFL_OK) break;
     if (c == 0) {  // observed iterations of the timed step
       std::vector<afl::SolveReport> reps(e->count);
       cudaMemcpy(reps.data(), e->d_rep_cur, sizeof(afl::SolveReport) * e->count,
@@ -659,17 +701,47 @@ afl_status afl_ensemble_autotune(afl_ensemble *e, int32_t *choice) {
     if (ms < best_ms) {
       best_ms = ms;
       best = static_cast<int>(c);
+      best_kz = 1;
+    }
+  }
+  for (int kz : {2, 4}) {
+    if (st != AFL_OK) break;
+    float ms = 0.0f;
+    st = time_one(cands[best], kz, &ms);
+    if (st == AFL_OK && ms < best_ms) {
+      best_ms = ms;
+      best_kz = kz;
     }
   }
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   restore();
-  for (void *s : snap) cudaFree(s);
-  if (st != AFL_OK) return st;
+  for (void *sp : snap) cudaFree(sp);
+  e->kz = kz0;  // the restored descriptors carry kz0
+  if (st != AFL_OK) {
+    set_tile_depth(e, kz0);  // the block table of the last candidate goes too
+    build_graph(e);
+    return st;
+  }
   ENS_TRY(build_systems(e, cands[best]));
+  ENS_TRY(set_tile_depth(e, best_kz));
   build_graph(e);
   e->tune_choice = best;
   if (choice) *choice = best;
+  return AFL_OK;
+}
+
+afl_status afl_ensemble_set_tile_depth(afl_ensemble *e, int32_t kz) {
+  if (!e) return fail(AFL_ERR_INVALID_ARGUMENT, "null ensemble");
+  if (kz != 1 && kz != 2 && kz != 4) return fail(AFL_ERR_INVALID_ARGUMENT, "tile depth must be 1, 2 or 4");
+  ENS_TRY(set_tile_depth(e, kz));
+  build_graph(e);
+  return AFL_OK;
+}
+
+afl_status afl_ensemble_tile_depth(const afl_ensemble *e, int32_t *kz) {
+  if (!e || !kz) return fail(AFL_ERR_INVALID_ARGUMENT, "null argument");
+  *kz = e->kz;
   return AFL_OK;
 }
 

@@ -1,9 +1,9 @@
 // afl_ensemble_kernels.cuh -- batched stage kernels for an ensemble of
 // independent smoke plumes of different grid sizes.
 //
-// One launch covers every instance: the plane blocks (32 x 8 cells of one z
-// plane, one 256-thread CTA each) of all instances are numbered consecutively and a block table maps a
-// CTA to its instance.  Each kernel calls the same per-cell functions as the
+// One launch covers every instance: the plane blocks (32 x 8 cells of kz z
+// planes, one 256-thread CTA each) of all instances are numbered
+// consecutively and a block table maps a CTA to its instance.  Each kernel calls the same per-cell functions as the
 // single-grid kernels of afl_stage.cuh, so an instance evolves exactly like a
 // single-grid solver with the same settings (up to the summation order of its
 // reductions).  Field pointers live in the device-side instance descriptors;
@@ -16,36 +16,40 @@
 
 namespace afl {
 
-template <typename T>
-__device__ __forceinline__ bool ens_cell(const EnsInstance<T> &d, int &i, int &j, int &k) {
+// The cells of this CTA: a 32 x 8 tile of d.kz consecutive z planes of its
+// instance (the tile depth is the tuner's choice); body(i, j, k) per cell.
+template <typename T, typename F>
+__device__ __forceinline__ void ens_cells(const EnsInstance<T> &d, F &&body) {
   const int local = blockIdx.x - d.blk_begin;
   const int gx = (d.g.nx + kTx - 1) / kTx, gy = (d.g.ny + kTy - 1) / kTy;
   const int bx = local % gx, t = local / gx;
   const int by = t % gy;
-  k = t / gy;
+  const int k0 = (t / gy) * d.kz;
   // 1-D CTAs of kTx*kTy threads: lane = x offset, warp = y offset
-  i = bx * kTx + static_cast<int>(threadIdx.x & (kTx - 1));
-  j = by * kTy + static_cast<int>(threadIdx.x / kTx);
-  return i < d.g.nx && j < d.g.ny;
+  const int i = bx * kTx + static_cast<int>(threadIdx.x & (kTx - 1));
+  const int j = by * kTy + static_cast<int>(threadIdx.x / kTx);
+  if (i >= d.g.nx || j >= d.g.ny) return;
+  const int k1 = min(k0 + d.kz, d.g.nz);
+  for (int k = k0; k < k1; ++k) body(i, j, k);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
     kb_advect_fwd(const EnsInstance<T> *inst, const int *blk_inst, int f) {
   const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
-  int i, j, k;
-  if (!ens_cell(d, i, j, k)) return;
-  cell_advect_fwd(d.g, d.fld[0], d.fld[1], d.fld[2], d.fld[f], d.tmp_fwd, d.scale_f, i, j, k);
+  ens_cells(d, [&](int i, int j, int k) {
+    cell_advect_fwd(d.g, d.fld[0], d.fld[1], d.fld[2], d.fld[f], d.tmp_fwd, d.scale_f, i, j, k);
+  });
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
     kb_advect_mc(const EnsInstance<T> *inst, const int *blk_inst, int f, double dissipation) {
   const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
-  int i, j, k;
-  if (!ens_cell(d, i, j, k)) return;
-  cell_advect_mc(d.g, d.fld[0], d.fld[1], d.fld[2], d.fld[f], d.tmp_fwd, d.tmp_out, d.scale_f,
-                 d.scale_b, T(dissipation), f >= 3 ? 1 : 0, i, j, k);
+  ens_cells(d, [&](int i, int j, int k) {
+    cell_advect_mc(d.g, d.fld[0], d.fld[1], d.fld[2], d.fld[f], d.tmp_fwd, d.tmp_out, d.scale_f,
+                   d.scale_b, T(dissipation), f >= 3 ? 1 : 0, i, j, k);
+  });
 }
 
 // The advected field becomes current; its old buffer becomes the next output.
@@ -61,10 +65,10 @@ __global__ void kb_swap(EnsInstance<T> *inst, int count, int f) {
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy) kb_curl(const EnsInstance<T> *inst, const int *blk_inst) {
   const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
-  int i, j, k;
-  if (!ens_cell(d, i, j, k)) return;
-  cell_curl(d.g, d.fld[0], d.fld[1], d.fld[2], d.curl[0], d.curl[1], d.curl[2], d.curl[3],
-            d.inv_2h, i, j, k);
+  ens_cells(d, [&](int i, int j, int k) {
+    cell_curl(d.g, d.fld[0], d.fld[1], d.fld[2], d.curl[0], d.curl[1], d.curl[2], d.curl[3],
+              d.inv_2h, i, j, k);
+  });
 }
 
 // Sphere source (density/temperature assignment) fused with the confinement
@@ -75,25 +79,25 @@ template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
     kb_source_confine_buoy(const EnsInstance<T> *inst, const int *blk_inst) {
   const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
-  int i, j, k;
-  if (!ens_cell(d, i, j, k)) return;
-  const int c = (k * d.g.ny + j) * d.g.nx + i;
-  T rho = d.fld[3][c], temp = d.fld[4][c];
-  if (d.src_on && i >= d.src_lo[0] && i <= d.src_hi[0] && j >= d.src_lo[1] &&
-      j <= d.src_hi[1] && k >= d.src_lo[2] && k <= d.src_hi[2]) {
-    const double dx = double(i) - d.src_c[0];
-    const double dy = double(j) - d.src_c[1];
-    const double dz = double(k) - d.src_c[2];
-    const double d2 = dx * dx + dy * dy + dz * dz;
-    if (d2 < d.src_r2) {
-      rho = T(d.src_rho);
-      temp = T(d.src_temp);
-      d.fld[3][c] = rho;
-      d.fld[4][c] = temp;
+  ens_cells(d, [&](int i, int j, int k) {
+    const int c = (k * d.g.ny + j) * d.g.nx + i;
+    T rho = d.fld[3][c], temp = d.fld[4][c];
+    if (d.src_on && i >= d.src_lo[0] && i <= d.src_hi[0] && j >= d.src_lo[1] &&
+        j <= d.src_hi[1] && k >= d.src_lo[2] && k <= d.src_hi[2]) {
+      const double dx = double(i) - d.src_c[0];
+      const double dy = double(j) - d.src_c[1];
+      const double dz = double(k) - d.src_c[2];
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 < d.src_r2) {
+        rho = T(d.src_rho);
+        temp = T(d.src_temp);
+        d.fld[3][c] = rho;
+        d.fld[4][c] = temp;
+      }
     }
-  }
-  cell_confine_buoy(d.g, d.fld[0], d.fld[1], d.fld[2], rho, temp, d.curl[0], d.curl[1],
-                    d.curl[2], d.curl[3], d.dt, d.eps_h, d.inv_2h, d.beta, d.alpha, i, j, k);
+    cell_confine_buoy(d.g, d.fld[0], d.fld[1], d.fld[2], rho, temp, d.curl[0], d.curl[1],
+                      d.curl[2], d.curl[3], d.dt, d.eps_h, d.inv_2h, d.beta, d.alpha, i, j, k);
+  });
 }
 
 // Right-hand side b = -h*(du+dv+dw) (src/fluid.rs:341-346), in f64.
@@ -101,27 +105,27 @@ template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
     kb_divergence(const EnsInstance<T> *inst, const int *blk_inst) {
   const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
-  int i, j, k;
-  if (!ens_cell(d, i, j, k)) return;
-  const int c = (k * d.g.ny + j) * d.g.nx + i;
-  double bv = 0.0;
-  if (interior(d.g, i, j, k)) {
-    const T *u = d.fld[0], *v = d.fld[1], *w = d.fld[2];
-    const double du = double(u[c + 1]) - double(u[c]);
-    const double dv = double(v[c + d.g.nx]) - double(v[c]);
-    const double dw = double(w[c + d.g.nxy]) - double(w[c]);
-    bv = -d.h * (du + dv + dw);
-  }
-  d.b[c] = bv;
+  ens_cells(d, [&](int i, int j, int k) {
+    const int c = (k * d.g.ny + j) * d.g.nx + i;
+    double bv = 0.0;
+    if (interior(d.g, i, j, k)) {
+      const T *u = d.fld[0], *v = d.fld[1], *w = d.fld[2];
+      const double du = double(u[c + 1]) - double(u[c]);
+      const double dv = double(v[c + d.g.nx]) - double(v[c]);
+      const double dw = double(w[c + d.g.nxy]) - double(w[c]);
+      bv = -d.h * (du + dv + dw);
+    }
+    d.b[c] = bv;
+  });
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
     kb_project(const EnsInstance<T> *inst, const int *blk_inst) {
   const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
-  int i, j, k;
-  if (!ens_cell(d, i, j, k)) return;
-  cell_project(d.g, d.fld[0], d.fld[1], d.fld[2], d.p, d.inv_h, i, j, k);
+  ens_cells(d, [&](int i, int j, int k) {
+    cell_project(d.g, d.fld[0], d.fld[1], d.fld[2], d.p, d.inv_h, i, j, k);
+  });
 }
 
 // compute_telemetry (src/fluid.rs:613-672): per-block partials of
@@ -131,16 +135,16 @@ __global__ void __launch_bounds__(kTx *kTy)
     kb_telemetry(const EnsInstance<T> *inst, const int *blk_inst, double *partials) {
   __shared__ double scratch[kWarps * 6];
   const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
-  int i, j, k;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   double peak = 0.0;
-  if (ens_cell(d, i, j, k) && interior(d.g, i, j, k)) {
+  ens_cells(d, [&](int i, int j, int k) {
+    if (!interior(d.g, i, j, k)) return;
     const Dims &g = d.g;
     const int c = (k * g.ny + j) * g.nx + i;
     const T *u = d.fld[0], *v = d.fld[1], *w = d.fld[2], *rho = d.fld[3];
     const double uc = u[c], vc = v[c], wc = w[c];
     const double u2 = uc * uc + vc * vc + wc * wc;
-    acc[0] = 0.5 * u2 * d.dv;
+    acc[0] += 0.5 * u2 * d.dv;
     const double inv_2h = d.inv_2h_d;
     const double dw_dy = (double(w[c + g.nx]) - double(w[c - g.nx])) * inv_2h;
     const double dv_dz = (double(v[c + g.nxy]) - double(v[c - g.nxy])) * inv_2h;
@@ -152,17 +156,17 @@ __global__ void __launch_bounds__(kTx *kTy)
     const double oy = du_dz - dw_dx;
     const double oz = dv_dx - du_dy;
     const double w2 = ox * ox + oy * oy + oz * oz;
-    acc[1] = 0.5 * w2 * d.dv;
-    peak = sqrt(w2);
+    acc[1] += 0.5 * w2 * d.dv;
+    peak = fmax(peak, sqrt(w2));
     const double r = rho[c];
     if (r > 1e-8) {
-      acc[2] = r * d.dv;
+      acc[2] += r * d.dv;
       const double wgt = r * d.dv;
-      acc[3] = (2.0 * (double(i) / double(g.nx - 1)) - 1.0) * wgt;
-      acc[4] = (2.0 * (double(j) / double(g.ny - 1)) - 1.0) * wgt;
-      acc[5] = (2.0 * (double(k) / double(g.nz - 1)) - 1.0) * wgt;
+      acc[3] += (2.0 * (double(i) / double(g.nx - 1)) - 1.0) * wgt;
+      acc[4] += (2.0 * (double(j) / double(g.ny - 1)) - 1.0) * wgt;
+      acc[5] += (2.0 * (double(k) / double(g.nz - 1)) - 1.0) * wgt;
     }
-  }
+  });
   block_sum<6>(acc, scratch);
   const double pk = block_max(peak, scratch);
   if (threadIdx.x == 0) {

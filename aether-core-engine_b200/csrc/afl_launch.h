@@ -204,6 +204,7 @@ struct EnsInstance {
   int src_lo[3], src_hi[3];   // clamped bounding box (src/fluid.rs:566-571 rule)
   double src_c[3], src_r2, src_rho, src_temp;
   int blk_begin, blk_count;   // plane blocks of this instance in the block table
+  int kz;                     // z planes per block (the tile depth chosen by the tuner)
 };
 
 template <typename T>

@@ -367,6 +367,7 @@ def time_ensemble(steps: int, torch, dist=None):
                          "cells": p.get("cells", 0), "run_s": p.get("run_seconds"),
                          "graph": p.get("info", {}).get("graph"),
                          "solver_ctas": p.get("info", {}).get("solver_ctas"),
+                         "tile_depth": p.get("info", {}).get("tile_depth"),
                          "autotune_choice": p.get("autotune_choice")} for p in parts]}
     if world == 1:
         single_s = 0.0

@@ -288,6 +288,11 @@ afl_status afl_ensemble_autotune(afl_ensemble *e, int32_t *choice);
  * budget, vector width, autotune choice (-1 = not tuned)} */
 afl_status afl_ensemble_info(const afl_ensemble *e, int32_t out[6]);
 afl_status afl_ensemble_instance_ctas(const afl_ensemble *e, int32_t *out, int count);
+/* Tile depth of the batched stage kernels: each CTA covers a 32 x 8 tile of
+ * kz consecutive z planes (1, 2 or 4).  afl_ensemble_autotune chooses it with
+ * the solver's CTA split; these set and read it directly. */
+afl_status afl_ensemble_set_tile_depth(afl_ensemble *e, int32_t kz);
+afl_status afl_ensemble_tile_depth(const afl_ensemble *e, int32_t *kz);
 /* The reference generator (src/rng.rs:21-88): n values of next_f64 after
  * skipping `skip` next_u64 draws from Rng::from_seed(seed). */
 afl_status afl_rng_f64(uint64_t seed, uint64_t skip, size_t n, double *out);

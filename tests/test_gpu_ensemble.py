@@ -61,6 +61,7 @@ def test_ensemble_autotune_restores_state(af):
     choice = a.autotune()
     assert choice in (0, 1, 2)
     assert a.info()["autotune_choice"] == choice
+    assert a.info()["tile_depth"] in (1, 2, 4)
     tel_a, _ = a.run(3)
     b = Ensemble(specs, precision=1)
     tel_b, _ = b.run(3)
@@ -101,3 +102,27 @@ def test_sharded_api_single_rank_is_the_batched_ensemble(af):
     np.testing.assert_array_equal(tel, ref_tel)
     assert [[i.iterations for i in row] for row in infos] == \
         [[i.iterations for i in row] for row in ref_infos]
+
+
+@pytest.mark.parametrize("kz", [2, 4])
+def test_tile_depth_does_not_change_the_evolution(af, kz):
+    """Stage tiles of 1, 2 or 4 z planes run the same per-cell code: the FP64
+    fields are identical; telemetry sums differ only in summation order."""
+    from aether_fluid.ensemble import Ensemble
+    specs = specs_small()
+    a = Ensemble(specs, precision=0)
+    tel_a, _ = a.run(3)
+    b = Ensemble(specs, precision=0)
+    b.set_tile_depth(kz)
+    assert b.info()["tile_depth"] == kz and b.info()["graph"]
+    tel_b, _ = b.run(3)
+    for m in range(len(specs)):
+        for f in FIELDS:
+            assert np.array_equal(a.field(m, f), b.field(m, f)), (m, f)
+    np.testing.assert_allclose(tel_b[:, :, 1:5], tel_a[:, :, 1:5], rtol=1e-12)
+    # switching back mid-run keeps going from the current state
+    b.set_tile_depth(1)
+    a.run(2)
+    b.run(2)
+    for m in range(len(specs)):
+        assert np.array_equal(a.field(m, "density"), b.field(m, "density"))
