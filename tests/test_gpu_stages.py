@@ -274,3 +274,31 @@ def test_resident_matches_streaming_at_full_size(af, shape, precision):
     assert rel_l2(out["resident"][0], out["streaming"][0]) <= tol
     fr, fs = out["resident"][1].final_residual, out["streaming"][1].final_residual
     assert abs(fr - fs) <= (1e-8 if precision == 0 else 1e-2) * fs
+
+
+# Shapes that reach every tile plan of the resident kernel (16 x TY columns,
+# CPT z cells per thread): TY = 16 needs a wide grid (TY = 4 and 8 would need
+# more tiles than SMs), ragged x/y tile edges, and a shallow grid.
+PLAN_SHAPES = {(160, 200, 32): 16, (100, 90, 120): 8, (130, 12, 7): 8, (37, 45, 29): 4}
+
+
+@pytest.mark.parametrize("shape", sorted(PLAN_SHAPES))
+@pytest.mark.parametrize("precision", [0, 1])
+def test_resident_tile_plans(af, shape, precision):
+    """Every tile plan solves the same system as the streaming kernel."""
+    nx, ny, nz = shape
+    st = seeded_state(shape, 67, 1.0)
+    out = {}
+    for kernel in ("streaming", "resident"):
+        g = af.FluidSolver3D(nx, ny, nz, precision=precision, poisson_kernel=KERNELS[kernel],
+                             mixed_inner_iters=40, mixed_max_refinements=1)
+        if kernel == "resident":
+            plan = g.poisson_plan()
+            assert plan["resident"] and plan["tile"][1] == PLAN_SHAPES[shape], plan
+        g.set_field("divergence", st["divergence"])
+        g.set_field("pressure", st["pressure"])
+        info = g.solve_poisson_conjugate_gradient(40)
+        assert info.iterations == 40, info
+        out[kernel] = g.get_field("pressure")
+    tol = 1e-10 if precision == 0 else 1e-4
+    assert rel_l2(out["resident"], out["streaming"]) <= tol
