@@ -28,25 +28,6 @@ __device__ __forceinline__ Vec<T, V> ldv(const T *p) {
   return *reinterpret_cast<const Vec<T, V> *>(p);
 }
 template <typename T, int V>
-__device__ __forceinline__ Vec<T, V> ldv_cg(const T *p) {
-  if constexpr (sizeof(T) * V == 16) {
-    const float4 x = __ldcg(reinterpret_cast<const float4 *>(p));
-    Vec<T, V> out;
-    memcpy(&out, &x, 16);
-    return out;
-  } else if constexpr (sizeof(T) * V == 8) {
-    const float2 x = __ldcg(reinterpret_cast<const float2 *>(p));
-    Vec<T, V> out;
-    memcpy(&out, &x, 8);
-    return out;
-  } else {
-    Vec<T, V> out;
-#pragma unroll
-    for (int a = 0; a < V; ++a) out.v[a] = __ldcg(p + a);
-    return out;
-  }
-}
-template <typename T, int V>
 __device__ __forceinline__ void stv(T *p, const Vec<T, V> &x) {
   *reinterpret_cast<Vec<T, V> *>(p) = x;
 }
@@ -82,13 +63,16 @@ struct DirF32 {
 
 // q = A dn over one run, dn formed on the fly from (r, dold); also returns the
 // run's dn (written by the caller) -- src/fluid.rs:356-394 per cell, with the
-// neighbour sum in the reference's order.
+// neighbour sum in the reference's order.  The loads may hit in L1: neighbour
+// rows of a CTA's runs are loaded by the same CTA.  r and dold were written
+// before the grid barrier that precedes this pass, and the barrier's acquire
+// and GPU-scope fence order these loads after those writes.
 template <typename T, int V, typename Dir>
 __device__ __forceinline__ void spmv_run(const Dims &g, const Run &ru, const T *r, const T *dold,
                                          bool first, T beta, Vec<T, V> &dn, Vec<T, V> &q) {
-  const Vec<T, V> rc = ldv_cg<T, V>(r + ru.c);
+  const Vec<T, V> rc = ldv<T, V>(r + ru.c);
   Vec<T, V> dc;
-  if (!first) dc = ldv_cg<T, V>(dold + ru.c);
+  if (!first) dc = ldv<T, V>(dold + ru.c);
 #pragma unroll
   for (int a = 0; a < V; ++a) dn.v[a] = Dir::make(first, rc.v[a], beta, first ? T(0) : dc.v[a]);
   const bool row_in = ru.j >= 1 && ru.j <= g.ny - 2 && ru.k >= 1 && ru.k <= g.nz - 2;
@@ -98,14 +82,14 @@ __device__ __forceinline__ void spmv_run(const Dims &g, const Run &ru, const T *
     return;
   }
   auto dn_at = [&](int c) {
-    const T rv = __ldcg(r + c);
-    return Dir::make(first, rv, beta, first ? T(0) : __ldcg(dold + c));
+    const T rv = r[c];
+    return Dir::make(first, rv, beta, first ? T(0) : dold[c]);
   };
   auto dn_vec = [&](int c) {
     Vec<T, V> out;
-    const Vec<T, V> rv = ldv_cg<T, V>(r + c);
+    const Vec<T, V> rv = ldv<T, V>(r + c);
     if (first) return rv;
-    const Vec<T, V> dv = ldv_cg<T, V>(dold + c);
+    const Vec<T, V> dv = ldv<T, V>(dold + c);
 #pragma unroll
     for (int a = 0; a < V; ++a) out.v[a] = Dir::make(false, rv.v[a], beta, dv.v[a]);
     return out;
