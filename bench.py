@@ -234,7 +234,7 @@ def time_large(torch, n: int = 256, steps: int = 100, seed: int = 1) -> dict:
 # profiles/k_cg_res_plume128.md and profiles/k_cg_stream_plume256.md).  Keyed by
 # (form, grid edge, resident kernel); other workloads report null.
 NCU_TRAFFIC = {("mixed_cg", 128, True): 42.9e6, ("fp64_cg", 128, True): 148.5e6,
-               ("mixed_cg", 256, False): 135.93e9, ("fp64_cg", 256, False): 268.68e9}
+               ("mixed_cg", 256, False): 135.93e9, ("fp64_cg", 256, False): 268.67e9}
 
 
 def measured_peak():
