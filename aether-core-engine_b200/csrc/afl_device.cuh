@@ -75,6 +75,27 @@ __device__ __forceinline__ Footprint<T> footprint(const Dims &g, T x, T y, T z) 
   return f;
 }
 
+// The interior cells of one red-black colour ((i + j + k) & 1 == color) by a
+// flat index q: rows (j, k) of the interior and, in each row, every second x
+// from the row's first interior cell of that colour.  `half` slots per row
+// cover the longer of the two parities; a slot past the row's last cell of the
+// colour is skipped.
+struct ColorWalk {
+  int half, rows_y, total;
+  __device__ explicit ColorWalk(const Dims &g)
+      : half((g.nx - 1) / 2), rows_y(g.ny - 2), total(((g.nx - 1) / 2) * (g.ny - 2) * (g.nz - 2)) {}
+  __device__ __forceinline__ bool cell(const Dims &g, int q, int color, int &i, int &j,
+                                       int &k) const {
+    const int row = q / half;
+    const int m = q - row * half;
+    const int kk = row / rows_y;
+    j = 1 + (row - kk * rows_y);
+    k = 1 + kk;
+    i = 1 + 2 * m + ((1 + j + k + color) & 1);
+    return i <= g.nx - 2;
+  }
+};
+
 // The footprint of the point (i, j, k) - (dx, dy, dz), a cell index moved by a
 // displacement.  In f64 this is footprint() of the moved position, the
 // reference's own expression (src/fluid.rs:160-162), bit for bit.

@@ -19,12 +19,13 @@ __global__ void __launch_bounds__(kBlock) k_rbsor_f64(SorArgs a, GridSync gs) {
   const int stride = gridDim.x * kBlock;
   double *p = a.p;
   const double omega = a.omega;
+  const ColorWalk walk(g);
   for (int sweep = 0; sweep < a.sweeps; ++sweep) {
     for (int color = 0; color < 2; ++color) {
-      for (int c = t0; c < g.n; c += stride) {
+      for (int q = t0; q < walk.total; q += stride) {
         int i, j, k;
-        decode(g, c, i, j, k);
-        if (!interior(g, i, j, k) || ((i + j + k) & 1) != color) continue;
+        if (!walk.cell(g, q, color, i, j, k)) continue;
+        const int c = (k * g.ny + j) * g.nx + i;
         double diag = 0.0, nb = 0.0;
         if (i > 1) { diag += 1.0; nb += p[c - 1]; }
         if (i + 2 < g.nx) { diag += 1.0; nb += p[c + 1]; }

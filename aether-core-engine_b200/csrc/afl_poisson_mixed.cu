@@ -37,12 +37,13 @@ __global__ void __launch_bounds__(kBlock) k_rbsor_mixed(SorMixedArgs a, GridSync
   }
   if (!grid_sync(gs)) return;
   const float omega = float(a.omega);
+  const ColorWalk walk(g);
   for (int sweep = 0; sweep < a.sweeps; ++sweep) {
     for (int color = 0; color < 2; ++color) {
-      for (int c = t0; c < g.n; c += stride) {
+      for (int q = t0; q < walk.total; q += stride) {
         int i, j, k;
-        decode(g, c, i, j, k);
-        if (!interior(g, i, j, k) || ((i + j + k) & 1) != color) continue;
+        if (!walk.cell(g, q, color, i, j, k)) continue;
+        const int c = (k * g.ny + j) * g.nx + i;
         float diag = 0.0f, nb = 0.0f;
         if (i > 1) { diag += 1.0f; nb += e[c - 1]; }
         if (i + 2 < g.nx) { diag += 1.0f; nb += e[c + 1]; }
