@@ -157,6 +157,20 @@ struct ResidentCgArgs {
   double rel_tol;
   SolveReport *report;
 };
+struct ResidentSorArgs {
+  Dims g;
+  int tiles_x, tiles_y;
+  double *p;            // f64 pressure (read, written)
+  const double *b;      // f64 right-hand side
+  float *e32;           // mixed: published tile-edge correction (n cells)
+  int sweeps;
+  double omega;
+  SolveReport *report;
+};
+// RB-SOR on the resident tile plan of the CG (the tile of one solved quantity
+// fits wherever the CG's does).
+int launch_sor_resident(const ResidentSorArgs &a, const ResidentPlan &plan, bool f64,
+                        const PersistentState &ps, cudaStream_t st);
 // False when the grid does not fit on chip (too many tiles, too much shared
 // memory, or more than 16 z cells per thread).
 bool plan_resident(const Dims &g, bool f64, ResidentPlan *plan);

@@ -317,6 +317,7 @@ struct Halo {
   static constexpr int kLanes = kRT / kPad;
   bool active;
   int col_c, col_s, k_first;
+  int par;  // (i + j) & 1 of the ring column: a ring cell's colour is (par + k) & 1
   __device__ Halo(const Dims &g, int tiles_x) {
     constexpr int SX = Plane<TY>::SX;
     const int q = threadIdx.x % kPad;
@@ -333,6 +334,7 @@ struct Halo {
     }
     const int i = bx0 + ii, j = by0 + jj;
     active = q < kPerPlane && i >= 0 && i < g.nx && j >= 0 && j < g.ny;
+    par = (i + j) & 1;
     col_c = j * g.nx + i;
     col_s = (jj + 1) * SX + ii + 1;
   }
@@ -347,6 +349,19 @@ struct Halo {
     if (!active) return;
 #pragma unroll 4
     for (int k = k_first; k < g.nz; k += kLanes) {
+      R &slot = D[k * SXY + col_s];
+      slot = value_at(k * g.nxy + col_c, slot);
+    }
+  }
+  // The red-black form: only ring cells of one colour ((i + j + k) & 1).
+  template <typename R, typename F>
+  __device__ __forceinline__ void fill_color(const Dims &g, R *D, int color,
+                                             const F &value_at) const {
+    constexpr int SXY = Plane<TY>::SXY;
+    if (!active) return;
+#pragma unroll 4
+    for (int k = k_first; k < g.nz; k += kLanes) {
+      if (((par + k) & 1) != color) continue;
       R &slot = D[k * SXY + col_s];
       slot = value_at(k * g.nxy + col_c, slot);
     }
@@ -635,6 +650,132 @@ __global__ void __launch_bounds__(kRT, 1)
   }
 }
 
+// ------------------------------------------------------------- RB-SOR ----
+// solve_poisson_gauss_seidel (src/fluid.rs:397-442) with the tile on chip: the
+// pressure (FP64) or the f32 correction (mixed) in shared memory with its halo
+// ring.  A half-sweep updates the cells of one colour in place (each reads only
+// the other colour), writes the tile-edge cells it changed to global memory,
+// and after one grid barrier the ring cells of that colour are reloaded from
+// there.  The FP64 update is the reference's expression with its neighbour
+// order, so a sweep equals the reference's bit for bit.
+template <typename R, int SX, int SXY, typename Cl>
+__device__ __forceinline__ void sor_terms(const Dims &g, const R *P, int s, const Cl &cl, int k,
+                                          R &nb, R &diag) {
+  const bool zl = k > 1, zh = k + 2 < g.nz;
+  nb = cl.xl ? P[s - 1] : R(0);
+  nb += cl.xh ? P[s + 1] : R(0);
+  nb += cl.yl ? P[s - SX] : R(0);
+  nb += cl.yh ? P[s + SX] : R(0);
+  nb += zl ? P[s - SXY] : R(0);
+  nb += zh ? P[s + SXY] : R(0);
+  diag = R(cl.diag_xy + int(zl) + int(zh));
+}
+
+template <int TY, int CPT>
+__global__ void __launch_bounds__(kRT, 1) k_sor_res_f64(ResidentSorArgs a, GridSync gs) {
+  using C = Cells<TY, CPT>;
+  extern __shared__ double Pbase[];
+  double *P = Pbase + C::SXY;  // one padding plane below plane 0
+  const Dims g = a.g;
+  const C cl(g, a.tiles_x);
+  const Halo<TY> halo(g, a.tiles_x);
+  double *p = a.p;
+#pragma unroll
+  for (int m = 0; m < CPT; ++m)
+    P[cl.s0 + m * C::SXY] = cl.valid(g, m) ? __ldcg(p + cl.c0 + m * g.nxy) : 0.0;
+  halo.fill_rolled(g, P, [&](int c, double) { return __ldcg(p + c); });
+  __syncthreads();
+  const double omega = a.omega;
+  const int par0 = (cl.i + cl.j + cl.k0) & 1;
+  for (int sweep = 0; sweep < a.sweeps; ++sweep) {
+    for (int color = 0; color < 2; ++color) {
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) {
+        if (((par0 + m) & 1) != color || !cl.interior(g, m)) continue;
+        const int s = cl.s0 + m * C::SXY;
+        const int c = cl.c0 + m * g.nxy;
+        double nb, diag;
+        sor_terms<double, C::SX, C::SXY>(g, P, s, cl, cl.k0 + m, nb, diag);
+        const double target = (__ldg(a.b + c) + nb) / diag;
+        const double v = (1.0 - omega) * P[s] + omega * target;
+        P[s] = v;
+        if (cl.edge) p[c] = v;
+      }
+      if (!grid_sync(gs)) return;
+      halo.fill_color(g, P, color, [&](int c, double) { return __ldcg(p + c); });
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < CPT; ++m)
+    if (cl.valid(g, m)) p[cl.c0 + m * g.nxy] = P[cl.s0 + m * C::SXY];
+  if (blockIdx.x == 0 && threadIdx.x == 0 && a.report) {
+    SolveReport rep{};
+    rep.iterations = a.sweeps;
+    *a.report = rep;
+  }
+}
+
+// Mixed RB-SOR: r = b - A p once in f64 (rounded to f32, kept in registers),
+// the sweeps on the f32 correction (A e = r from e = 0, the same linear
+// iteration as sweeping p), then p += e in f64.  Published edge values go
+// through a.e32.
+template <int TY, int CPT>
+__global__ void __launch_bounds__(kRT, 1) k_sor_res_mixed(ResidentSorArgs a, GridSync gs) {
+  using C = Cells<TY, CPT>;
+  extern __shared__ float Ebase[];
+  float *E = Ebase + C::SXY;
+  const Dims g = a.g;
+  const C cl(g, a.tiles_x);
+  const Halo<TY> halo(g, a.tiles_x);
+  double *p = a.p;
+  float *epub = a.e32;
+  float rb[CPT];
+#pragma unroll
+  for (int m = 0; m < CPT; ++m) {
+    rb[m] = 0.0f;
+    E[cl.s0 + m * C::SXY] = 0.0f;
+    if (!cl.valid(g, m)) continue;
+    const int c = cl.c0 + m * g.nxy;
+    const double ap = cl.interior(g, m) ? lap_global(g, p, c, cl.i, cl.j, cl.k0 + m) : 0.0;
+    rb[m] = float(__ldg(a.b + c) - ap);
+  }
+  halo.fill_rolled(g, E, [&](int, float) { return 0.0f; });
+  __syncthreads();
+  const float omega = float(a.omega);
+  const int par0 = (cl.i + cl.j + cl.k0) & 1;
+  for (int sweep = 0; sweep < a.sweeps; ++sweep) {
+    for (int color = 0; color < 2; ++color) {
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) {
+        if (((par0 + m) & 1) != color || !cl.interior(g, m)) continue;
+        const int s = cl.s0 + m * C::SXY;
+        float nb, diag;
+        sor_terms<float, C::SX, C::SXY>(g, E, s, cl, cl.k0 + m, nb, diag);
+        const float target = (rb[m] + nb) / diag;
+        const float v = (1.0f - omega) * E[s] + omega * target;
+        E[s] = v;
+        if (cl.edge) epub[cl.c0 + m * g.nxy] = v;
+      }
+      if (!grid_sync(gs)) return;
+      halo.fill_color(g, E, color, [&](int c, float) { return __ldcg(epub + c); });
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < CPT; ++m) {
+    if (!cl.valid(g, m)) continue;
+    const int c = cl.c0 + m * g.nxy;
+    p[c] = p[c] + double(E[cl.s0 + m * C::SXY]);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && a.report) {
+    SolveReport rep{};
+    rep.iterations = a.sweeps;
+    rep.refinements = 1;
+    *a.report = rep;
+  }
+}
+
 // ---------------------------------------------------------------- dispatch --
 using KernelFn = void (*)(ResidentCgArgs, GridSync, TagSync);
 
@@ -654,7 +795,55 @@ KernelFn kernel_for(bool f64, int ty, int cpt) {
   return nullptr;
 }
 
+using SorFn = void (*)(ResidentSorArgs, GridSync);
+
+template <int TY, int CPT>
+SorFn pick_sor(bool f64) {
+  return f64 ? &k_sor_res_f64<TY, CPT> : &k_sor_res_mixed<TY, CPT>;
+}
+
+SorFn sor_kernel_for(bool f64, int ty, int cpt) {
+#define AFL_SOR_CASE(TY_, CPT_) \
+  if (ty == TY_ && cpt == CPT_) return pick_sor<TY_, CPT_>(f64);
+  AFL_SOR_CASE(4, 1) AFL_SOR_CASE(4, 2) AFL_SOR_CASE(4, 4) AFL_SOR_CASE(4, 8) AFL_SOR_CASE(4, 16)
+  AFL_SOR_CASE(8, 1) AFL_SOR_CASE(8, 2) AFL_SOR_CASE(8, 4) AFL_SOR_CASE(8, 8) AFL_SOR_CASE(8, 16)
+  AFL_SOR_CASE(16, 1) AFL_SOR_CASE(16, 2) AFL_SOR_CASE(16, 4) AFL_SOR_CASE(16, 8)
+  AFL_SOR_CASE(16, 16)
+#undef AFL_SOR_CASE
+  return nullptr;
+}
+
 }  // namespace
+
+int launch_sor_resident(const ResidentSorArgs &a, const ResidentPlan &plan, bool f64,
+                        const PersistentState &ps, cudaStream_t st) {
+  SorFn fn = sor_kernel_for(f64, plan.ty, plan.cpt);
+  if (!fn) return -static_cast<int>(cudaErrorInvalidConfiguration);
+  const int blocks = plan.tiles_x * plan.tiles_y;
+  if (blocks > ps.max_blocks) return -static_cast<int>(cudaErrorInvalidConfiguration);
+  // one tile of the solved quantity: f64 pressure or f32 correction
+  const size_t tile = resident_smem_bytes(a.g, plan.ty, plan.cpt, true) / sizeof(double);
+  const int smem = static_cast<int>(tile * (f64 ? sizeof(double) : sizeof(float)));
+  cudaError_t err = cudaFuncSetAttribute(reinterpret_cast<const void *>(fn),
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (err != cudaSuccess) return -static_cast<int>(err);
+  cudaMemsetAsync(ps.count, 0, sizeof(unsigned int), st);
+  cudaMemsetAsync(ps.gen, 0, sizeof(unsigned int), st);
+  cudaMemsetAsync(ps.abort_flag, 0, sizeof(int), st);
+  ResidentSorArgs args = a;
+  args.tiles_x = plan.tiles_x;
+  args.tiles_y = plan.tiles_y;
+  GridSync gs;
+  gs.count = ps.count;
+  gs.gen = ps.gen;
+  gs.abort_flag = ps.abort_flag;
+  gs.nblocks = static_cast<unsigned int>(blocks);
+  gs.timeout_ns = ps.timeout_ns;
+  void *params[] = {&args, &gs};
+  err = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(fn), dim3(blocks), dim3(kRT),
+                                    params, static_cast<size_t>(smem), st);
+  return err == cudaSuccess ? blocks : -static_cast<int>(err);
+}
 
 size_t resident_smem_bytes(const Dims &g, int ty, int cpt, bool f64) {
   // FP64: the direction tile.  Mixed: direction and q = A d tiles (f32).

@@ -338,6 +338,23 @@ afl_status stage_solve(afl_solver *s, int kind, int iters, afl::SolveReport *rep
     a.rel_tol = s->params.cg_rel_tol;
     a.report = rep;
     blocks = afl::launch_cg_resident(a, s->resident, f64, s->ps, s->stream);
+  } else if (kind != AFL_POISSON_CG && s->resident_ok &&
+             (s->params.poisson_kernel == AFL_POISSON_KERNEL_RESIDENT ||
+              (s->params.poisson_kernel == AFL_POISSON_KERNEL_AUTO &&
+               s->precision != AFL_PRECISION_FP64))) {
+    // RB-SOR on chip: the automatic choice for the mixed form only.  The FP64
+    // sweep re-reads its f64 right-hand side from L2 every half-sweep (no room
+    // on chip beside the f64 tile), and the streaming colour walk is faster.
+    const bool f64 = s->precision == AFL_PRECISION_FP64;
+    afl::ResidentSorArgs a{};
+    a.g = g;
+    a.p = s->p;
+    a.b = s->b;
+    a.e32 = f64 ? nullptr : static_cast<float *>(s->cg[0]);
+    a.sweeps = iters;
+    a.omega = s->params.sor_omega;
+    a.report = rep;
+    blocks = afl::launch_sor_resident(a, s->resident, f64, s->ps, s->stream);
   } else if (s->precision == AFL_PRECISION_FP64) {
     if (kind == AFL_POISSON_CG) {
       afl::CgArgs a{g, s->p, s->b, static_cast<double *>(s->cg[0]),

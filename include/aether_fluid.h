@@ -73,9 +73,12 @@ typedef enum afl_precision {
   AFL_PRECISION_MIXED = 1
 } afl_precision;
 
-/* CG kernel choice.  AUTO: the on-chip resident kernel when the grid fits
- * (tiles <= SMs, tile + halo in shared memory), else the streaming kernel.
- * The two differ only in the summation order of the inner products. */
+/* Poisson kernel choice.  CG, AUTO: the on-chip resident kernel when the grid
+ * fits (tiles <= SMs, tile + halo in shared memory), else the streaming
+ * kernel; the two differ only in the summation order of the inner products.
+ * RB-SOR, AUTO: the resident kernel for the mixed form when the grid fits,
+ * else the streaming sweep; RESIDENT selects the resident sweep for FP64 too
+ * (same result bit for bit, since a colour reads only the other colour). */
 typedef enum afl_poisson_kernel {
   AFL_POISSON_KERNEL_AUTO = 0,
   AFL_POISSON_KERNEL_STREAMING = 1,
@@ -117,7 +120,7 @@ typedef struct afl_params {
   double mixed_inner_rel_tol; /* MIXED: inner f32 CG relative tolerance
                                  (default 1e-4) */
   int32_t mixed_max_refinements; /* MIXED: max outer passes (default 8) */
-  int32_t poisson_kernel; /* afl_poisson_kernel: which CG kernel runs */
+  int32_t poisson_kernel; /* afl_poisson_kernel: which Poisson kernel runs */
   double reserved_f64[4];
 } afl_params;
 

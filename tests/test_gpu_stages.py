@@ -302,3 +302,25 @@ def test_resident_tile_plans(af, shape, precision):
         out[kernel] = g.get_field("pressure")
     tol = 1e-10 if precision == 0 else 1e-4
     assert rel_l2(out["resident"], out["streaming"]) <= tol
+
+
+@pytest.mark.parametrize("shape", sorted(PLAN_SHAPES) + [(128, 128, 128)])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_resident_sor_matches_streaming(af, shape, precision):
+    """RB-SOR on the resident tiles equals the streaming sweep: bit for bit in
+    FP64 (each colour reads only the other colour, so the visiting order does
+    not matter); the mixed form to f32 rounding."""
+    nx, ny, nz = shape
+    st = seeded_state(shape, 71, 1.0)
+    out = {}
+    for kernel in ("streaming", "resident"):
+        g = af.FluidSolver3D(nx, ny, nz, precision=precision, poisson_kernel=KERNELS[kernel])
+        g.set_params(solver_kind=1, sor_omega=1.7)
+        g.set_field("divergence", st["divergence"])
+        g.set_field("pressure", st["pressure"])
+        g.solve_poisson_gauss_seidel(25)
+        out[kernel] = g.get_field("pressure")
+    if precision == 0:
+        assert np.array_equal(out["resident"], out["streaming"])
+    else:
+        assert rel_l2(out["resident"], out["streaming"]) <= 1e-5
