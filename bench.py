@@ -477,8 +477,8 @@ def time_medium(torch, n_rays: int = 1 << 20, cpu_rays: int = 4000) -> dict:
     o = np.tile([0.0, 2.4, 9.0], (n_rays, 1))
     target = rng.uniform(lo, hi, size=(n_rays, 3))
     rays = np.column_stack([o, target - o, np.full(n_rays, 1e-4), np.full(n_rays, 20.0)])
-    m.transmittance(rays[:4096], 1)          # warm-up
-    m.sample_interaction(rays[:4096], 1)
+    m.transmittance(rays, 1)                 # warm-up at full size: staging buffers grown
+    m.sample_interaction(rays, 1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     tr = m.transmittance(rays, 7)
