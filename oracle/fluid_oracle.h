@@ -6,7 +6,7 @@
  * queries of `FluidMedium` (src/fluid.rs:687-874) and of the
  * SplitMix64/Xoshiro256++ generator (src/rng.rs:5-88) of
  * vanovri/aether-core-engine.  Only tests/, __graft_entry__.smoke() and the
- * CPU-baseline leg of bench.py may load it, and only as the checker.  The
+ * CPU-baseline leg of bench.py may load it, and only to check results.  The
  * product path (libaether_fluid.so) never links or calls it.
  *
  * Parity pin: the reference is Rust and cannot be built in this image, so the

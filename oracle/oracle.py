@@ -3,7 +3,7 @@
 The oracle is the f64 C++ restatement of the reference smoke solver
 (`src/fluid.rs:23-673`, `src/rng.rs:5-88` of vanovri/aether-core-engine) in
 `oracle/fluid_oracle.cpp`.  Only `tests/`, `__graft_entry__.smoke()` and the
-CPU-baseline leg of `bench.py` import this module, and only as the checker;
+CPU-baseline leg of `bench.py` import this module, and only to check results;
 the product library never calls it.
 """
 from __future__ import annotations
