@@ -1,11 +1,11 @@
 // afl_poisson_stream.cu -- streaming persistent CG for grids that do not fit
 // on chip (256^3 and up), vectorised along x.
 //
-// Each thread handles runs of V consecutive x cells (V = 2 doubles or 4
-// floats: 16-byte loads) and walks the runs of the whole grid with a stride
-// of the CTA grid, so every array is streamed from HBM once per phase while
-// the y/z neighbour planes of a run are served by L2; grids whose nx is not a
-// multiple of the vector width use V = 1.  The solve is one cooperative launch
+// Each thread handles runs of V consecutive x cells (the widest of 4 / 2 / 1
+// doubles or 8 / 4 / 1 floats that divides nx) and walks the runs of the
+// whole grid with a stride of the CTA grid, so every array is streamed from
+// HBM once per phase while the y neighbour rows of a run hit in L1 and the z
+// neighbour planes in L2.  The solve is one cooperative launch
 // with two bounded grid barriers per iteration; the direction update
 // d = r + beta*d (src/fluid.rs:483-485) is formed on the fly inside the next
 // matrix-vector product (double-buffered d).  Built with -fmad=false: the FP64
@@ -536,26 +536,37 @@ int launch_cg_multi(const MultiCgSystem *d_sys, const int *d_cta_inst, int total
 }
 
 int persistent_blocks_stream() {
-  const int a = blocks_of(&k_cg_stream_f64<1>), b = blocks_of(&k_cg_stream_f64<2>);
-  const int c = blocks_of(&k_cg_stream_mixed<1>), d = blocks_of(&k_cg_stream_mixed<4>);
-  return a > b ? (a > c ? (a > d ? a : d) : (c > d ? c : d)) : (b > c ? (b > d ? b : d) : (c > d ? c : d));
+  const int counts[] = {blocks_of(&k_cg_stream_f64<1>), blocks_of(&k_cg_stream_f64<2>),
+                        blocks_of(&k_cg_stream_f64<4>), blocks_of(&k_cg_stream_mixed<1>),
+                        blocks_of(&k_cg_stream_mixed<4>), blocks_of(&k_cg_stream_mixed<8>)};
+  int most = 0;
+  for (int c : counts) most = c > most ? c : most;
+  return most;
 }
 
+// Cells per run: the widest of 4 / 2 / 1 doubles or 8 / 4 / 1 floats that
+// divides nx (wider runs keep more bytes in flight per thread).
 int stream_vector_width(const Dims &g, bool f64) {
-  const int v = f64 ? 2 : 4;
-  return g.nx % v == 0 ? v : 1;
+  const int widths[2][3] = {{8, 4, 1}, {4, 2, 1}};
+  for (int v : widths[f64 ? 1 : 0])
+    if (g.nx % v == 0) return v;
+  return 1;
 }
 
 int launch_cg_stream_f64(const CgArgs &a, const PersistentState &ps, cudaStream_t st) {
-  if (stream_vector_width(a.g, true) == 2)
-    return launch_persistent(&k_cg_stream_f64<2>, a, ps, 2, st);
-  return launch_persistent(&k_cg_stream_f64<1>, a, ps, 2, st);
+  switch (stream_vector_width(a.g, true)) {
+    case 4: return launch_persistent(&k_cg_stream_f64<4>, a, ps, 2, st);
+    case 2: return launch_persistent(&k_cg_stream_f64<2>, a, ps, 2, st);
+    default: return launch_persistent(&k_cg_stream_f64<1>, a, ps, 2, st);
+  }
 }
 
 int launch_cg_stream_mixed(const MixedCgArgs &a, const PersistentState &ps, cudaStream_t st) {
-  if (stream_vector_width(a.g, false) == 4)
-    return launch_persistent(&k_cg_stream_mixed<4>, a, ps, 3, st);
-  return launch_persistent(&k_cg_stream_mixed<1>, a, ps, 3, st);
+  switch (stream_vector_width(a.g, false)) {
+    case 8: return launch_persistent(&k_cg_stream_mixed<8>, a, ps, 3, st);
+    case 4: return launch_persistent(&k_cg_stream_mixed<4>, a, ps, 3, st);
+    default: return launch_persistent(&k_cg_stream_mixed<1>, a, ps, 3, st);
+  }
 }
 
 }  // namespace afl
