@@ -453,8 +453,11 @@ __global__ void __launch_bounds__(kST) k_cg_stream_f64(CgArgs a, GridSync gs, Ri
   cg_stream_f64_body<V>(a, gs, pr, blockIdx.x, gridDim.x, scratch);
 }
 
+// 8-float runs otherwise take 127 registers and fit 2 CTAs per SM; capped at
+// 80 (a few bytes of spill) they fit 3, which keeps more runs in flight.
 template <int V>
-__global__ void __launch_bounds__(kST) k_cg_stream_mixed(MixedCgArgs a, GridSync gs, Ring3 pr) {
+__global__ void __launch_bounds__(kST, (V == 8 ? 3 : 1))
+    k_cg_stream_mixed(MixedCgArgs a, GridSync gs, Ring3 pr) {
   __shared__ double scratch[(kST / 32) * 3 + 4];
   cg_stream_mixed_body<V>(a, gs, pr, blockIdx.x, gridDim.x, scratch);
 }
