@@ -8,7 +8,10 @@
 // neighbour planes in L2.  The solve is one cooperative launch
 // with two bounded grid barriers per iteration; the direction update
 // d = r + beta*d (src/fluid.rs:483-485) is formed on the fly inside the next
-// matrix-vector product (double-buffered d).  Built with -fmad=false: the FP64
+// matrix-vector product (double-buffered d), and for a single large grid
+// q = A d is recomputed in the update pass rather than stored; passes
+// alternate their walking direction so each starts in L2.  Built with
+// -fmad=false: the FP64
 // path keeps the reference's un-fused expressions (the mixed path writes its
 // FMAs explicitly).
 #include "afl_launch.h"
@@ -47,6 +50,12 @@ __device__ __forceinline__ Run decode_run(const Dims &g, int run) {
   r.j = row - r.k * g.ny;
   r.c = row * g.nx + r.i0;
   return r;
+}
+
+// The last of a thread's runs t0, t0 + stride, ... (t0 - stride when it has
+// none), where a backward walk starts.
+__device__ __forceinline__ int last_run(int t0, int stride, int runs) {
+  return t0 < runs ? t0 + ((runs - 1 - t0) / stride) * stride : t0 - stride;
 }
 
 // Direction value at a cell, formed from r and the previous direction with
@@ -114,6 +123,40 @@ __device__ __forceinline__ void spmv_run(const Dims &g, const Run &ru, const T *
     if (zl) { diag += T(1); nb += zm.v[a]; }
     if (zh) { diag += T(1); nb += zp.v[a]; }
     q.v[a] = diag * dn.v[a] - nb;
+  }
+}
+
+// q = A d over one run from the stored direction d, with spmv_run's
+// arithmetic and neighbour order, so it reproduces that pass's q bit for bit.
+template <typename T, int V>
+__device__ __forceinline__ void lap_run(const Dims &g, const Run &ru, const T *d,
+                                        const Vec<T, V> &dc, Vec<T, V> &q) {
+  const bool row_in = ru.j >= 1 && ru.j <= g.ny - 2 && ru.k >= 1 && ru.k <= g.nz - 2;
+  if (!row_in) {
+#pragma unroll
+    for (int a = 0; a < V; ++a) q.v[a] = T(0);
+    return;
+  }
+  const T left = ru.i0 > 0 ? d[ru.c - 1] : T(0);
+  const T right = ru.i0 + V < g.nx ? d[ru.c + V] : T(0);
+  const Vec<T, V> ym = ldv<T, V>(d + ru.c - g.nx), yp = ldv<T, V>(d + ru.c + g.nx);
+  const Vec<T, V> zm = ldv<T, V>(d + ru.c - g.nxy), zp = ldv<T, V>(d + ru.c + g.nxy);
+  const bool yl = ru.j > 1, yh = ru.j + 2 < g.ny, zl = ru.k > 1, zh = ru.k + 2 < g.nz;
+#pragma unroll
+  for (int a = 0; a < V; ++a) {
+    const int i = ru.i0 + a;
+    if (i < 1 || i > g.nx - 2) {
+      q.v[a] = T(0);
+      continue;
+    }
+    T diag = T(0), nb = T(0);
+    if (i > 1) { diag += T(1); nb += a == 0 ? left : dc.v[a - 1]; }
+    if (i + 2 < g.nx) { diag += T(1); nb += a == V - 1 ? right : dc.v[a + 1]; }
+    if (yl) { diag += T(1); nb += ym.v[a]; }
+    if (yh) { diag += T(1); nb += yp.v[a]; }
+    if (zl) { diag += T(1); nb += zm.v[a]; }
+    if (zh) { diag += T(1); nb += zp.v[a]; }
+    q.v[a] = diag * dc.v[a] - nb;
   }
 }
 
@@ -192,7 +235,16 @@ struct Ring3 {
 // ------------------------------------------------------------------ FP64 ----
 // The solve run by CTA `vblock` of `vgrid` CTAs working on this system (the
 // whole launch for a single grid, a slice of it in the batched launch).
-template <int V>
+//
+// SINGLE (one grid larger than L2, the whole launch):
+//  - the update pass recomputes q = A d from the stored direction instead of
+//    storing q in the matrix-vector pass and reading it back (8 / 4 bytes
+//    less per cell written and read);
+//  - the matrix-vector pass walks its runs backward and the other passes
+//    forward, so each pass starts on the runs the previous one touched last,
+//    which are still in L2.
+// The batched systems fit in L2, where neither pays; they keep the plain form.
+template <int V, bool SINGLE>
 __device__ __forceinline__ void cg_stream_f64_body(const CgArgs &a, const GridSync &gs,
                                                    const Ring3 &pr, int vblock, int vgrid,
                                                    double *scratch) {
@@ -243,12 +295,13 @@ __device__ __forceinline__ void cg_stream_f64_body(const CgArgs &a, const GridSy
     while (it < a.max_iters) {
       const bool first = it == 0;
       double acc[1] = {0.0};
-      for (int run = t0; run < runs; run += stride) {
+      for (int run = SINGLE ? last_run(t0, stride, runs) : t0;
+           SINGLE ? run >= t0 : run < runs; run += SINGLE ? -stride : stride) {
         const Run ru = decode_run<V>(g, run);
         Vec<double, V> dn, qv;
         spmv_run<double, V, DirF64<double>>(g, ru, r, dold, first, beta, dn, qv);
         stv<double, V>(dnew + ru.c, dn);
-        stv<double, V>(q + ru.c, qv);
+        if (!SINGLE) stv<double, V>(q + ru.c, qv);
 #pragma unroll
         for (int e = 0; e < V; ++e) acc[0] += dn.v[e] * qv.v[e];
       }
@@ -261,10 +314,13 @@ __device__ __forceinline__ void cg_stream_f64_body(const CgArgs &a, const GridSy
       const double alpha = delta / dq[0];
       double acc2[1] = {0.0};
       for (int run = t0; run < runs; run += stride) {
-        const int c = decode_run<V>(g, run).c;
+        const Run ru = decode_run<V>(g, run);
+        const int c = ru.c;
         Vec<double, V> pv = ldv<double, V>(p + c);
         const Vec<double, V> dv = ldv<double, V>(dnew + c);
-        const Vec<double, V> qv = ldv<double, V>(q + c);
+        Vec<double, V> qv;
+        if (!SINGLE) qv = ldv<double, V>(q + c);
+        else lap_run<double, V>(g, ru, dnew, dv, qv);
         Vec<double, V> rv = ldv<double, V>(r + c);
 #pragma unroll
         for (int e = 0; e < V; ++e) {
@@ -306,7 +362,7 @@ __device__ __forceinline__ void cg_stream_f64_body(const CgArgs &a, const GridSy
 }
 
 // ----------------------------------------------------------------- mixed ----
-template <int V>
+template <int V, bool SINGLE>
 __device__ __forceinline__ void cg_stream_mixed_body(const MixedCgArgs &a, const GridSync &gs,
                                                      const Ring3 &pr, int vblock, int vgrid,
                                                      double *scratch) {
@@ -370,12 +426,13 @@ __device__ __forceinline__ void cg_stream_mixed_body(const MixedCgArgs &a, const
       const bool first = it == 0;
       const float bf = float(beta);
       double acc[1] = {0.0};
-      for (int run = t0; run < runs; run += stride) {
+      for (int run = SINGLE ? last_run(t0, stride, runs) : t0;
+           SINGLE ? run >= t0 : run < runs; run += SINGLE ? -stride : stride) {
         const Run ru = decode_run<V>(g, run);
         Vec<float, V> dn, qv;
         spmv_run<float, V, DirF32>(g, ru, r, dold, first, bf, dn, qv);
         stv<float, V>(dnew + ru.c, dn);
-        stv<float, V>(q + ru.c, qv);
+        if (!SINGLE) stv<float, V>(q + ru.c, qv);
 #pragma unroll
         for (int x = 0; x < V; ++x) acc[0] += double(dn.v[x]) * double(qv.v[x]);
       }
@@ -388,10 +445,13 @@ __device__ __forceinline__ void cg_stream_mixed_body(const MixedCgArgs &a, const
       const float af = float(delta / dq[0]);
       double acc2[1] = {0.0};
       for (int run = t0; run < runs; run += stride) {
-        const int c = decode_run<V>(g, run).c;
+        const Run ru = decode_run<V>(g, run);
+        const int c = ru.c;
         Vec<float, V> ev = ldv<float, V>(e + c);
         const Vec<float, V> dv = ldv<float, V>(dnew + c);
-        const Vec<float, V> qv = ldv<float, V>(q + c);
+        Vec<float, V> qv;
+        if (!SINGLE) qv = ldv<float, V>(q + c);
+        else lap_run<float, V>(g, ru, dnew, dv, qv);
         Vec<float, V> rv = ldv<float, V>(r + c);
 #pragma unroll
         for (int x = 0; x < V; ++x) {
@@ -417,7 +477,8 @@ __device__ __forceinline__ void cg_stream_mixed_body(const MixedCgArgs &a, const
       dnew = t;
     }
     // p += e (f64), then the true residual again
-    for (int run = t0; run < runs; run += stride) {
+    for (int run = SINGLE ? last_run(t0, stride, runs) : t0;
+           SINGLE ? run >= t0 : run < runs; run += SINGLE ? -stride : stride) {
       const int c = decode_run<V>(g, run).c;
       Vec<double, V> pv = ldv<double, V>(p + c);
       const Vec<float, V> ev = ldv<float, V>(e + c);
@@ -447,19 +508,22 @@ __device__ __forceinline__ void cg_stream_mixed_body(const MixedCgArgs &a, const
   }
 }
 
+// 4-double runs with the recomputed q take ~93 registers (2 CTAs per SM);
+// capped at 80 they fit 3 (256^3: 323 -> 359 Mcell-steps/s).
 template <int V>
-__global__ void __launch_bounds__(kST) k_cg_stream_f64(CgArgs a, GridSync gs, Ring3 pr) {
+__global__ void __launch_bounds__(kST, (V == 4 ? 3 : 1))
+    k_cg_stream_f64(CgArgs a, GridSync gs, Ring3 pr) {
   __shared__ double scratch[(kST / 32) * 3 + 4];
-  cg_stream_f64_body<V>(a, gs, pr, blockIdx.x, gridDim.x, scratch);
+  cg_stream_f64_body<V, true>(a, gs, pr, blockIdx.x, gridDim.x, scratch);
 }
 
 // 8-float runs otherwise take 127 registers and fit 2 CTAs per SM; capped at
-// 80 (a few bytes of spill) they fit 3, which keeps more runs in flight.
+// 80 they fit 3, which keeps more runs in flight.
 template <int V>
 __global__ void __launch_bounds__(kST, (V == 8 ? 3 : 1))
     k_cg_stream_mixed(MixedCgArgs a, GridSync gs, Ring3 pr) {
   __shared__ double scratch[(kST / 32) * 3 + 4];
-  cg_stream_mixed_body<V>(a, gs, pr, blockIdx.x, gridDim.x, scratch);
+  cg_stream_mixed_body<V, true>(a, gs, pr, blockIdx.x, gridDim.x, scratch);
 }
 
 // Many independent solves in one cooperative launch: CTA b works on system
@@ -475,10 +539,10 @@ __global__ void __launch_bounds__(kST) k_cg_stream_multi(const MultiCgSystem *sy
   const Ring3 pr{s.partials, (F64 ? 2 : 3) * s.ctas};
   if constexpr (F64) {
     const CgArgs a = s.f64;
-    cg_stream_f64_body<V>(a, s.gs, pr, vblock, s.ctas, scratch);
+    cg_stream_f64_body<V, false>(a, s.gs, pr, vblock, s.ctas, scratch);
   } else {
     const MixedCgArgs a = s.mixed;
-    cg_stream_mixed_body<V>(a, s.gs, pr, vblock, s.ctas, scratch);
+    cg_stream_mixed_body<V, false>(a, s.gs, pr, vblock, s.ctas, scratch);
   }
 }
 
