@@ -243,7 +243,8 @@ struct Ring3 {
 //  - the matrix-vector pass walks its runs backward and the other passes
 //    forward, so each pass starts on the runs the previous one touched last,
 //    which are still in L2.
-// The batched systems fit in L2, where neither pays; they keep the plain form.
+// The batched solves (many small grids side by side) measured slower in this
+// form (48-plume ensemble 560 -> 537 Mcell-steps/s) and keep the plain one.
 template <int V, bool SINGLE>
 __device__ __forceinline__ void cg_stream_f64_body(const CgArgs &a, const GridSync &gs,
                                                    const Ring3 &pr, int vblock, int vgrid,
