@@ -509,19 +509,24 @@ __device__ __forceinline__ void cg_stream_mixed_body(const MixedCgArgs &a, const
   }
 }
 
-// 4-double runs with the recomputed q take ~93 registers (2 CTAs per SM);
-// capped at 80 they fit 3 (256^3: 323 -> 359 Mcell-steps/s).
+// Register caps (CTAs per SM).  Uncapped, 4-double runs with the recomputed
+// q take ~93 registers (2 CTAs per SM), 2- and 1-double runs 108 / 90;
+// capped at 80 / 64 they fit 3 / 4 without spilling more than a few bytes
+// (256^3: 323 -> 359; 258 x 256^2: 243 -> 310; 257 x 256^2: 172 -> 234
+// Mcell-steps/s).
 template <int V>
-__global__ void __launch_bounds__(kST, (V == 4 ? 3 : 1))
+__global__ void __launch_bounds__(kST, (V == 4 ? 3 : 4))
     k_cg_stream_f64(CgArgs a, GridSync gs, Ring3 pr) {
   __shared__ double scratch[(kST / 32) * 3 + 4];
   cg_stream_f64_body<V, true>(a, gs, pr, blockIdx.x, gridDim.x, scratch);
 }
 
-// 8-float runs otherwise take 127 registers and fit 2 CTAs per SM; capped at
-// 80 they fit 3, which keeps more runs in flight.
+// Uncapped, 8-float runs take 127 registers (2 CTAs per SM), 4- and 1-float
+// runs ~150 (1 CTA per SM); capped at 80 / 64 they fit 3 / 4 without
+// spilling (256^3: 602 -> 635; 260 x 256^2: 287 -> 612; 257 x 256^2:
+// 106 -> 275 Mcell-steps/s).
 template <int V>
-__global__ void __launch_bounds__(kST, (V == 8 ? 3 : 1))
+__global__ void __launch_bounds__(kST, (V == 8 ? 3 : 4))
     k_cg_stream_mixed(MixedCgArgs a, GridSync gs, Ring3 pr) {
   __shared__ double scratch[(kST / 32) * 3 + 4];
   cg_stream_mixed_body<V, true>(a, gs, pr, blockIdx.x, gridDim.x, scratch);
