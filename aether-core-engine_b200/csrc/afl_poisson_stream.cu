@@ -536,10 +536,11 @@ __global__ void __launch_bounds__(kST, (V == 8 ? 3 : 4))
 // cta_inst[b] as its (b - first CTA of that system)-th CTA; each system has its
 // own barrier, partials and stopping decisions, so systems finish at their
 // own iteration counts.
-// Capped at 64 registers (4 CTAs per SM instead of 3, no more spill than at
-// 80): the 48-plume ensemble 560 -> 592 Mcell-steps/s.
+// Capped at 48 registers: 5 CTAs per SM instead of 3 (at 80) for ~70 bytes of
+// spill; the 48-plume ensemble 560 -> 596 (4 per SM) -> 605-616 Mcell-steps/s.
+// At 6 per SM (40 registers) the spill doubles.
 template <int V, bool F64>
-__global__ void __launch_bounds__(kST, 4) k_cg_stream_multi(const MultiCgSystem *sys,
+__global__ void __launch_bounds__(kST, 5) k_cg_stream_multi(const MultiCgSystem *sys,
                                                             const int *cta_inst) {
   __shared__ double scratch[(kST / 32) * 3 + 4];
   const MultiCgSystem &s = sys[cta_inst[blockIdx.x]];
