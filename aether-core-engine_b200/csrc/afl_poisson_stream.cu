@@ -537,8 +537,8 @@ __global__ void __launch_bounds__(kST, (V == 8 ? 3 : 4))
 // own barrier, partials and stopping decisions, so systems finish at their
 // own iteration counts.
 // Capped at 48 registers: 5 CTAs per SM instead of 3 (at 80) for ~70 bytes of
-// spill; the 48-plume ensemble 560 -> 596 (4 per SM) -> 605-616 Mcell-steps/s.
-// At 6 per SM (40 registers) the spill doubles.
+// spill; the 48-plume ensemble 560 -> 596 (4 per SM) -> 605-624 Mcell-steps/s
+// (FP64 ensemble: 338 -> 342).  At 6 per SM (40 registers) the spill doubles.
 template <int V, bool F64>
 __global__ void __launch_bounds__(kST, 5) k_cg_stream_multi(const MultiCgSystem *sys,
                                                             const int *cta_inst) {
