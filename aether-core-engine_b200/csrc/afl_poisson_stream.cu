@@ -363,6 +363,8 @@ __device__ __forceinline__ void cg_stream_f64_body(const CgArgs &a, const GridSy
 }
 
 // ----------------------------------------------------------------- mixed ----
+// f32 CG on the correction e inside f64 iterative refinement; SINGLE as for
+// the FP64 body.
 template <int V, bool SINGLE>
 __device__ __forceinline__ void cg_stream_mixed_body(const MixedCgArgs &a, const GridSync &gs,
                                                      const Ring3 &pr, int vblock, int vgrid,
@@ -479,7 +481,7 @@ __device__ __forceinline__ void cg_stream_mixed_body(const MixedCgArgs &a, const
     }
     // p += e (f64), then the true residual again
     for (int run = SINGLE ? last_run(t0, stride, runs) : t0;
-           SINGLE ? run >= t0 : run < runs; run += SINGLE ? -stride : stride) {
+         SINGLE ? run >= t0 : run < runs; run += SINGLE ? -stride : stride) {
       const int c = decode_run<V>(g, run).c;
       Vec<double, V> pv = ldv<double, V>(p + c);
       const Vec<float, V> ev = ldv<float, V>(e + c);
