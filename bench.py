@@ -741,7 +741,8 @@ def run_reference(args):
               f"(CG iters {iters}); C++ restatement of the reference's single-threaded "
               f"Rust solver (no Rust toolchain here), {cpu_model()}")
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus,  # the launch's GPU count; the timed work ran on 1 CPU core
         "steps": steps, "warmup": warm, "ms_per_step": el * 1e3 / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded velocity noise, sphere source)",
