@@ -390,9 +390,14 @@ constexpr int kScratch = kRW * 3 + 3 + 3;
 // solve_poisson_conjugate_gradient (src/fluid.rs:445-493) with the relative
 // tolerance extension.  d in shared memory, r in registers, p in global memory
 // (updated once per iteration, never read by the operator).
+// The arguments are __grid_constant__: they stay in the constant bank, which
+// leaves the compiler's 64 registers to the f64 residuals (128^3: 395 -> 413
+// Mcell-steps/s).  The mixed kernel keeps plain arguments, which measured
+// better for it.
 template <int TY, int CPT>
 __global__ void __launch_bounds__(kRT, 1)
-    k_cg_res_f64(ResidentCgArgs a, GridSync gs, TagSync ts) {
+    k_cg_res_f64(const __grid_constant__ ResidentCgArgs a, const __grid_constant__ GridSync gs,
+                 const __grid_constant__ TagSync ts) {
   using C = Cells<TY, CPT>;
   extern __shared__ double Dbase[];
   double *D = Dbase + C::SXY;  // one padding plane below plane 0
