@@ -103,6 +103,8 @@ struct afl_adjoint {
   double *partials = nullptr, *scal = nullptr;
   afl::SolveReport *rep = nullptr;
   afl::PersistentState ps{};
+  afl::ResidentPlan res{};  // on-chip CG tiles, when the grid fits
+  bool resident = false;
   std::vector<std::array<double *, 6>> ckpt;
   std::vector<Rec> rec;
   // adjoint work arrays
@@ -148,10 +150,25 @@ afl_status copy(afl_adjoint *a, double *dst, const double *src) {
   return AFL_OK;
 }
 
+// The FP64 CG of afl_solve_cg (warm start from x): the on-chip resident
+// kernel when the grid fits, else the streaming one.
 afl_status solve(afl_adjoint *a, double *x, const double *rhs, long *iters) {
-  afl::CgArgs args{a->g, x, rhs, a->cg[0], a->cg[1], a->cg[2], a->cg[3],
-                   a->params.solver_iters, a->params.cg_rel_tol, a->rep};
-  const int used = afl::launch_cg_f64(args, a->ps, a->stream);
+  int used;
+  if (a->resident) {
+    afl::ResidentCgArgs ra{};
+    ra.g = a->g;
+    ra.p = x;
+    ra.b = rhs;
+    ra.rpub = a->cg[0];
+    ra.max_iters = a->params.solver_iters;
+    ra.rel_tol = a->params.cg_rel_tol;
+    ra.report = a->rep;
+    used = afl::launch_cg_resident(ra, a->res, true, a->ps, a->stream);
+  } else {
+    afl::CgArgs args{a->g, x, rhs, a->cg[0], a->cg[1], a->cg[2], a->cg[3],
+                     a->params.solver_iters, a->params.cg_rel_tol, a->rep};
+    used = afl::launch_cg_f64(args, a->ps, a->stream);
+  }
   if (used <= 0) return cuda_fail(static_cast<cudaError_t>(-used), "CG launch");
   afl::SolveReport r{};
   ADJ_CUDA(cudaMemcpyAsync(&r, a->rep, sizeof r, cudaMemcpyDeviceToHost, a->stream));
@@ -382,12 +399,16 @@ afl_status afl_adjoint_create(size_t nx, size_t ny, size_t nz, const afl_params 
   a->ps.count = static_cast<unsigned int *>(v);
   a->ps.gen = a->ps.count + 1;
   a->ps.abort_flag = reinterpret_cast<int *>(a->ps.count + 2);
-  if (cudaMalloc(&v, sizeof(double) * 6 * static_cast<size_t>(maxb)) != cudaSuccess)
+  // partials of the streaming CG (2 x 2 per CTA) or tagged slots of the resident one
+  // (2 buffers x 2 words x up to 3 values per tile)
+  if (cudaMalloc(&v, sizeof(double) * 12 * static_cast<size_t>(maxb)) != cudaSuccess)
     return bail(fail(AFL_ERR_OUT_OF_MEMORY, "CG partials"));
   a->allocs.push_back(v);
   a->ps.partials = static_cast<double *>(v);
   a->ps.max_blocks = maxb;
   a->ps.timeout_ns = 5000000000ull;
+  a->resident = afl::plan_resident(a->g, true, &a->res) &&
+                a->res.tiles_x * a->res.tiles_y <= maxb;
   // one segment of recorded steps
   a->rec.resize(static_cast<size_t>(a->k));
   for (Rec &R : a->rec) {
