@@ -22,13 +22,14 @@ def _p(a):
 class Adjoint:
     def __init__(self, nx, ny, nz, center, radius, eps=0.3, beta=0.4, alpha=0.08,
                  cg_rel_tol=1e-10, solver_iters=2000, checkpoint_every=8, density=1.0,
-                 temperature=1.0):
+                 temperature=1.0, poisson_kernel=0):
         lib = _lib.load()
         self._lib = lib
         p = _lib.default_params()
         p.vorticity_eps, p.buoyancy_beta, p.gravity_alpha = eps, beta, alpha
         p.solver_kind, p.solver_iters, p.cg_rel_tol = 0, solver_iters, cg_rel_tol
         p.source_kind = 1
+        p.poisson_kernel = poisson_kernel
         for a in range(3):
             p.sphere_center[a] = float(center[a])
         p.sphere_radius = float(radius)

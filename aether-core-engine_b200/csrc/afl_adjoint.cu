@@ -407,8 +407,15 @@ afl_status afl_adjoint_create(size_t nx, size_t ny, size_t nz, const afl_params 
   a->ps.partials = static_cast<double *>(v);
   a->ps.max_blocks = maxb;
   a->ps.timeout_ns = 5000000000ull;
-  a->resident = afl::plan_resident(a->g, true, &a->res) &&
-                a->res.tiles_x * a->res.tiles_y <= maxb;
+  // The Poisson kernel follows params->poisson_kernel as afl_create's does:
+  // AUTO takes the on-chip resident CG when the grid fits, STREAMING never,
+  // RESIDENT always (an error when the grid does not fit).
+  const bool fits = afl::plan_resident(a->g, true, &a->res) &&
+                    a->res.tiles_x * a->res.tiles_y <= maxb;
+  if (params->poisson_kernel == AFL_POISSON_KERNEL_RESIDENT && !fits)
+    return bail(fail(AFL_ERR_INVALID_ARGUMENT,
+                     "the grid does not fit the resident CG kernel"));
+  a->resident = fits && params->poisson_kernel != AFL_POISSON_KERNEL_STREAMING;
   // one segment of recorded steps
   a->rec.resize(static_cast<size_t>(a->k));
   for (Rec &R : a->rec) {

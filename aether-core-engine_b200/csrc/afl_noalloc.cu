@@ -1,14 +1,17 @@
 // afl_noalloc.cu -- a CG pressure solve for callers that cannot allocate.
 //
-// Some callers may not call cudaMalloc at all: code that records its work
-// into a CUDA graph (allocation is not a capturable operation), real-time or
-// render threads that must never block on the driver's allocator, and hosts
-// whose device memory is owned entirely by their own pool or arena (a game
-// engine's or a renderer's budgeted heap), where a hidden allocation by a
-// library breaks the budget.  For them afl_solve_cg_noalloc runs the same
-// persistent FP64 CG kernel as afl_solve_cg on device buffers the caller
-// already owns, and takes the solver's working memory from one fixed array
-// compiled into this library instead of allocating it.
+// Some callers may not call cudaMalloc at all: real-time or render threads
+// that must never block on the driver's allocator (cudaMalloc can wait for
+// the device and takes driver locks), and hosts whose device memory is owned
+// entirely by their own pool or arena (a game engine's or a renderer's
+// budgeted heap), where a hidden allocation by a library breaks the budget.
+// For them afl_solve_cg_noalloc runs the streaming persistent FP64 CG kernel
+// (the kernel afl_solve_cg runs with AFL_POISSON_KERNEL_STREAMING; its AUTO
+// choice may run the on-chip resident kernel instead, whose sums are ordered
+// differently) on device buffers the caller already owns, and takes the
+// solver's working memory from one fixed array compiled into this library
+// instead of allocating it.  The call synchronises its stream before it
+// returns, to read the solve's report.
 //
 // The array below is that working memory.  Every GPU that loads the library
 // holds it (kNoAllocBytes, about 8.1 MiB) until the process exits.  All calls
@@ -75,11 +78,15 @@ extern "C" afl_status afl_solve_cg_noalloc(const double *d_rhs, double *d_pressu
     return fail(AFL_ERR_INVALID_ARGUMENT, "null device buffer");
   if (nx < 6 || ny < 6 || nz < 6)
     return fail(AFL_ERR_INVALID_ARGUMENT, "every grid dimension must be >= 6");
-  if (nx * ny * nz > kNoAllocMaxCells) {
-    char msg[200];
+  // Each dimension is at least 6, so a grid within the limit has every
+  // dimension below kNoAllocMaxCells / 36; checking them one by one first
+  // keeps the product from wrapping around.
+  if (nx > kNoAllocMaxCells / 36 || ny > kNoAllocMaxCells / 36 || nz > kNoAllocMaxCells / 36 ||
+      nx * ny * nz > kNoAllocMaxCells) {
+    char msg[240];
     snprintf(msg, sizeof msg,
-             "grid of %zu cells exceeds the no-allocation limit of %zu cells (64^3); "
-             "use afl_solve_cg on a solver handle", nx * ny * nz, kNoAllocMaxCells);
+             "grid %zux%zux%zu exceeds the no-allocation limit of %zu cells (64^3); "
+             "use afl_solve_cg on a solver handle", nx, ny, nz, kNoAllocMaxCells);
     return fail(AFL_ERR_INVALID_ARGUMENT, msg);
   }
   if (max_iters < 0 || !(rel_tol >= 0.0))

@@ -10,8 +10,11 @@ projection with the pressure solve; advection of density and temperature;
 telemetry).
 
 Forms measured in one run:
-  mixed_cg  (headline `value`)  f32 stencils/SpMV, f64 dots, f64 refinement to 1e-6
-  fp64_cg                      the plain f64 drop-in, CG to 1e-6 (max 200)
+  fp64_cg   (headline `value`)  the plain f64 drop-in, CG to 1e-6 (max 200): the
+                               same arithmetic as the f64 reference arm
+  mixed_cg                     f32 stencils/SpMV, f64 dots, f64 refinement to 1e-6
+                               (in `variants`, with its speed-up over fp64_cg and
+                               its relative L2 difference from it)
   fp64_sor / mixed_sor         red-black SOR omega = 1.7, 80 sweeps per step
 Each form runs W untimed warm-up steps, is re-initialised (outside the timed
 region) and then times exactly K steps from the initial state on the device
@@ -46,7 +49,6 @@ sys.path.insert(0, os.path.join(ROOT, "aether-core-engine_b200"))
 METRIC = ("Mcell-steps/s 128³: FP32+FP64-refine vs FP64 GPU @1e-5 err; "
           "adjoint/fwd ratio")
 UNIT = "Mcell-steps/s"
-WORKLOAD = "smoke plume 128x128x128, sphere source r=10 at (64,12.8,64), seed 0, dt=0.5h"
 
 
 def parse():
@@ -59,7 +61,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=0, help="velocity-noise seed (default 0)")
     ap.add_argument("--poisson-kernel", type=int, default=0,
                     help="CG kernel: 0 auto, 1 streaming, 2 on-chip resident")
-    ap.add_argument("--forms", default="mixed_cg,fp64_cg,fp64_sor,mixed_sor")
+    ap.add_argument("--forms", default="fp64_cg,mixed_cg,fp64_sor,mixed_sor")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true",
@@ -75,6 +77,8 @@ def parse():
                     help="finite-difference directions checked against the adjoint")
     ap.add_argument("--cpu-seconds", type=float, default=20.0,
                     help="target length of the bounded CPU sample")
+    ap.add_argument("--reference-seconds", type=float, default=150.0,
+                    help="time bound of the reference arm's timed steps")
     return ap.parse_args()
 
 
@@ -88,6 +92,18 @@ def plume_for(form: str, n: int, seed: int | None = None):
     if form.endswith("sor"):
         return Plume(n, n, n, 200, seed=seed, solver="sor", iters=80)
     return Plume(n, n, n, 200, seed=seed)
+
+
+def bench_config(form: str, n: int, world: int) -> dict:
+    """The `config` object of a bench line; both arms print the same one."""
+    p = plume_for(form, n)
+    c = ",".join(f"{x:g}" for x in p.center)
+    workload = (f"smoke plume {n}x{n}x{n}, sphere source r={p.radius:g} at ({c}), "
+                f"seed {p.seed}, dt=0.5h")
+    return {"workload": workload, "form": form, "grid": [n] * 3,
+            "solver": "CG rel 1e-6 max 200" if "cg" in form else "RB-SOR omega 1.7 x 80",
+            "parallelism": f"replicas x{world}",
+            "l2": "state larger than L2 (no flush between steps)"}
 
 
 # ---------------------------------------------------------------- clocks -----
@@ -229,12 +245,14 @@ def time_large(torch, n: int = 256, steps: int = 100, seed: int = 1) -> dict:
     return out
 
 
-# DRAM bytes per launch of the Poisson kernel (dram__bytes_read.sum +
-# dram__bytes_write.sum from one ncu capture of the same workload:
-# profiles/k_cg_res_plume128.md and profiles/k_cg_stream_plume256.md).  Keyed by
-# (form, grid edge, resident kernel); other workloads report null.
-NCU_TRAFFIC = {("mixed_cg", 128, True): 42.9e6, ("fp64_cg", 128, True): 148.5e6,
-               ("mixed_cg", 256, False): 135.93e9, ("fp64_cg", 256, False): 268.67e9}
+# DRAM bytes per launch of the Poisson kernel: dram__bytes_read.sum +
+# dram__bytes_write.sum of one ncu capture of that kernel on the same workload
+# (one solve of the plume at that grid edge).  Keyed by (kernel, grid edge);
+# any other kernel or workload reports null.  A capture is not taken inside
+# this script: ncu replays each launch many times, so its figure is recorded
+# here beside the kernel it belongs to.
+NCU_TRAFFIC = {("k_cg_res_f64", 128): 148.5e6, ("k_cg_res_mixed", 128): 42.9e6,
+               ("k_cg_stream_f64", 256): 268.67e9, ("k_cg_stream_mixed", 256): 135.93e9}
 
 
 def measured_peak():
@@ -626,6 +644,11 @@ def run_ours(args):
         pois_ms, pois_calls = head["stages"]["poisson"]
         pois_bytes = poisson_bytes(cells, headline, head["infos"])
         achieved = pois_bytes / pois_calls / (pois_ms / pois_calls / 1e3) / 1e9
+        pois_kernel = {"mixed_cg": ("k_cg_res_mixed", "k_cg_stream_mixed"),
+                       "fp64_cg": ("k_cg_res_f64", "k_cg_stream_f64"),
+                       "fp64_sor": ("k_rbsor_f64",) * 2,
+                       "mixed_sor": ("k_rbsor_mixed",) * 2}[headline][
+                           0 if head["plan"]["resident"] else 1]
         variants = {}
         for form, r in results.items():
             its = [i.iterations for i in r["infos"]]
@@ -666,21 +689,16 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f32+f64" if headline.startswith("mixed") else "f64",
             "data": "synthetic (seeded velocity noise, sphere source)",
-            "config": {"workload": WORKLOAD, "form": headline, "grid": [args.n] * 3,
-                       "solver": "CG rel 1e-6 max 200" if "cg" in headline else
-                       "RB-SOR omega 1.7 x 80", "parallelism": f"replicas x{world}",
-                       "l2": "state larger than L2 (no flush between steps)"},
+            "config": bench_config(headline, args.n, world),
             "gpu_launches": int(head["launches"]),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": NCU_TRAFFIC.get((headline, args.n,
-                                                     bool(head["plan"]["resident"]))),
+                         "traffic": NCU_TRAFFIC.get((pois_kernel, args.n)),
+                         "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                            "of one capture of this kernel on this workload"
+                                            if (pois_kernel, args.n) in NCU_TRAFFIC else None),
                          "algorithmic_bytes_per_launch": pois_bytes / pois_calls,
-                         "kernel": {"mixed_cg": ("k_cg_res_mixed", "k_cg_stream_mixed"),
-                                    "fp64_cg": ("k_cg_res_f64", "k_cg_stream_f64"),
-                                    "fp64_sor": ("k_rbsor_f64",) * 2,
-                                    "mixed_sor": ("k_rbsor_mixed",) * 2}[headline][
-                                        0 if head["plan"]["resident"] else 1],
+                         "kernel": pois_kernel,
                          "note": ("on-chip resident solve: achieved is algorithmic bytes over "
                                   "kernel time (an effective bandwidth); DRAM traffic is the "
                                   "measured ncu figure" if head["plan"]["resident"] else
@@ -711,11 +729,17 @@ def run_ours(args):
 
 
 def run_reference(args):
+    """The reference arm: the CPU oracle (a C++ restatement of the reference's
+    single-threaded Rust solver, which has no toolchain in this image) on the
+    same workload, form and config as our arm, on one host core.  It runs W
+    untimed warm-up steps, re-initialises the plume (untimed) and times
+    exactly K steps from the initial state, as our arm does; a step is one
+    full f64 plume step (about 3 s at 128^3).  Should K steps exceed the time
+    bound, it stops early and reports the steps it timed."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    warm = min(args.warmup, 1)
-    budget = max(args.cpu_seconds, 10.0)
+    bound = max(args.reference_seconds, 10.0)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.build()
@@ -723,21 +747,25 @@ def run_reference(args):
     s = O.OracleSolver(p.nx, p.ny, p.nz)
     s.set_params(vorticity_eps=p.eps, buoyancy_beta=p.beta, gravity_alpha=p.alpha,
                  solver_kind=O.CG, solver_iters=p.iters, cg_rel_tol=p.rel_tol)
-    s.init_velocity_noise(p.seed)
     s.set_sphere_source(p.center, p.radius)
-    for n in range(warm):
-        s.step(p.dt, n * p.dt)
+    s.init_velocity_noise(p.seed)
+    t0 = time.perf_counter()
+    warm = 0
+    while warm < args.warmup and time.perf_counter() - t0 < bound / 4:
+        s.step(p.dt, warm * p.dt)
+        warm += 1
+    s.init_velocity_noise(p.seed)  # back to the initial state (untimed)
     t0 = time.perf_counter()
     steps, iters = 0, []
     while steps < args.steps:
-        s.step(p.dt, (warm + steps) * p.dt)
+        s.step(p.dt, steps * p.dt)
         iters.append(s.last_cg_iters())
         steps += 1
-        if time.perf_counter() - t0 >= budget:
+        if time.perf_counter() - t0 >= bound:
             break
     el = time.perf_counter() - t0
     value = p.cells * steps / el / 1e6
-    sample = (f"steps {warm}..{warm + steps - 1} of the 128^3 plume in f64 on 1 core "
+    sample = (f"steps 0..{steps - 1} of the {args.n}^3 plume in f64 on 1 core "
               f"(CG iters {iters}); C++ restatement of the reference's single-threaded "
               f"Rust solver (no Rust toolchain here), {cpu_model()}")
     line = {
@@ -746,7 +774,7 @@ def run_reference(args):
         "steps": steps, "warmup": warm, "ms_per_step": el * 1e3 / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded velocity noise, sphere source)",
-        "config": {"workload": WORKLOAD, "form": "reference f64 CG", "grid": [args.n] * 3},
+        "config": bench_config("fp64_cg", args.n, args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,

@@ -371,19 +371,20 @@ afl_status afl_medium_sample_interaction(afl_medium *m, const afl_ray *rays, siz
 
 /* ---- a pressure solve that allocates nothing --------------------------------
  * No counterpart in the reference.  For callers that may not allocate device
- * memory -- code recorded into a CUDA graph, real-time/render threads that
- * must not block on the allocator, hosts whose device memory is one budgeted
- * pool -- this runs the FP64 CG of afl_solve_cg (same kernel, same stopping
- * rules, warm start from *d_pressure) on device buffers the caller owns:
- * d_rhs (read) and d_pressure (read and written), nx*ny*nz doubles each, x
- * fastest.  Its working memory is a fixed array inside the library (about
- * 8.1 MiB, held on every GPU that loads the library until exit), so grids
- * larger than 262144 cells (64^3) are rejected with AFL_ERR_INVALID_ARGUMENT.
- * The first call on each device looks up that array's device address (with
- * the device current) and should come before any stream capture.  All calls
- * share the array: calls whose work overlaps on one GPU race and must be
- * ordered by the caller.  Runs on `stream` (a cudaStream_t, NULL = legacy
- * default) and synchronises it before returning; info may be NULL; errors are
+ * memory -- real-time/render threads that must not block on the driver's
+ * allocator, hosts whose device memory is one budgeted pool -- this runs the
+ * streaming FP64 CG kernel (the one afl_solve_cg runs with
+ * AFL_POISSON_KERNEL_STREAMING; same stopping rules, warm start from
+ * *d_pressure) on device buffers the caller owns: d_rhs (read) and d_pressure
+ * (read and written), nx*ny*nz doubles each, x fastest.  Its working memory is
+ * a fixed array inside the library (about 8.1 MiB, held on every GPU that
+ * loads the library until exit), so grids larger than 262144 cells (64^3) are
+ * rejected with AFL_ERR_INVALID_ARGUMENT.  The first call on each device looks
+ * up that array's device address (with the device current) and should come
+ * before any stream capture.  All calls share the array: calls whose work
+ * overlaps on one GPU race and must be ordered by the caller.  Runs on
+ * `stream` (a cudaStream_t, NULL = legacy default) and synchronises it before
+ * returning, to read the solve's report; info may be NULL; errors are
  * reported through afl_last_error(). */
 afl_status afl_solve_cg_noalloc(const double *d_rhs, double *d_pressure, size_t nx, size_t ny,
                                 size_t nz, int max_iters, double rel_tol, void *stream,

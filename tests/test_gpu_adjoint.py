@@ -60,11 +60,11 @@ CG_ITERS = 4000
 EPS = 1e-6
 
 
-def make(af, shape, k=4, shift=0.0):
+def make(af, shape, k=4, shift=0.0, poisson_kernel=0):
     from aether_fluid.adjoint import Adjoint
     c, r = source(shape, shift)
     return Adjoint(*shape, center=c, radius=r, checkpoint_every=k, cg_rel_tol=CG_REL_TOL,
-                   solver_iters=CG_ITERS)
+                   solver_iters=CG_ITERS, poisson_kernel=poisson_kernel)
 
 
 @pytest.fixture(scope="module")
@@ -147,6 +147,28 @@ def test_checkpoint_interval_does_not_change_the_gradient(af, case, k):
     g = a.backward(rho - tgt)
     for got, ref in zip(g, case["grads"]):
         assert rel_l2(got, ref) <= 1e-9
+
+
+def test_poisson_kernel_choice_gives_the_same_gradient(af, case):
+    """The forward and adjoint pressure solves run on the kernel the params
+    name (AUTO takes the resident one at this grid).  The streaming and the
+    resident kernel give iteration counts within one per solve of each other
+    and the same gradient: they differ only in the order of the inner-product
+    sums."""
+    x, dt, tgt = case["x"], case["dt"], case["tgt"]
+    runs = {}
+    for kernel in (1, 2):   # STREAMING, RESIDENT
+        a = make(af, SHAPE, poisson_kernel=kernel)
+        rho = a.forward(*x, STEPS, dt)
+        g = a.backward(rho - tgt)
+        runs[kernel] = (rho, g, a.stats())
+        a.close()
+    (rs, gs, ss), (rr, gr, sr) = runs[1], runs[2]
+    assert rel_l2(rs, rr) <= 1e-10 and rel_l2(rr, case["rho"]) <= 1e-12
+    assert abs(ss["forward_cg_iters"] - sr["forward_cg_iters"]) <= 2 * STEPS
+    assert abs(ss["adjoint_cg_iters"] - sr["adjoint_cg_iters"]) <= STEPS
+    for a, b, want in zip(gs, gr, case["grads"]):
+        assert rel_l2(a, b) <= 1e-8 and rel_l2(b, want) <= 1e-10
 
 
 def test_forward_matches_oracle_and_oracle_fd(af, oracle, case):
