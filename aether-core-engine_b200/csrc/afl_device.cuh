@@ -59,19 +59,38 @@ struct Footprint {
   T tx, ty, tz;
 };
 
+// The same footprint with the corner as three indices (the fused stage
+// kernels test whether it lies inside their shared-memory tile).
 template <typename T>
-__device__ __forceinline__ Footprint<T> footprint(const Dims &g, T x, T y, T z) {
+struct Footprint3 {
+  int i, j, k;  // corner (i0, j0, k0)
+  T tx, ty, tz;
+  __device__ __forceinline__ int base(const Dims &g) const { return (k * g.ny + j) * g.nx + i; }
+};
+
+template <typename T>
+__device__ __forceinline__ Footprint3<T> footprint3(const Dims &g, T x, T y, T z) {
   const T xc = rs_clamp(x, T(0.5), T(g.nx) - T(1.500001));
   const T yc = rs_clamp(y, T(0.5), T(g.ny) - T(1.500001));
   const T zc = rs_clamp(z, T(0.5), T(g.nz) - T(1.500001));
-  const int i0 = static_cast<int>(floor(xc));
-  const int j0 = static_cast<int>(floor(yc));
-  const int k0 = static_cast<int>(floor(zc));
+  Footprint3<T> f;
+  f.i = static_cast<int>(floor(xc));
+  f.j = static_cast<int>(floor(yc));
+  f.k = static_cast<int>(floor(zc));
+  f.tx = xc - T(f.i);
+  f.ty = yc - T(f.j);
+  f.tz = zc - T(f.k);
+  return f;
+}
+
+template <typename T>
+__device__ __forceinline__ Footprint<T> footprint(const Dims &g, T x, T y, T z) {
+  const Footprint3<T> f3 = footprint3(g, x, y, z);
   Footprint<T> f;
-  f.base = (k0 * g.ny + j0) * g.nx + i0;
-  f.tx = xc - T(i0);
-  f.ty = yc - T(j0);
-  f.tz = zc - T(k0);
+  f.base = f3.base(g);
+  f.tx = f3.tx;
+  f.ty = f3.ty;
+  f.tz = f3.tz;
   return f;
 }
 
@@ -100,9 +119,9 @@ struct ColorWalk {
 // displacement.  In f64 this is footprint() of the moved position, the
 // reference's own expression (src/fluid.rs:160-162), bit for bit.
 template <typename T>
-__device__ __forceinline__ Footprint<T> footprint_at(const Dims &g, int i, int j, int k, T dx,
-                                                     T dy, T dz) {
-  return footprint(g, T(i) - dx, T(j) - dy, T(k) - dz);
+__device__ __forceinline__ Footprint3<T> footprint3_at(const Dims &g, int i, int j, int k, T dx,
+                                                       T dy, T dz) {
+  return footprint3(g, T(i) - dx, T(j) - dy, T(k) - dz);
 }
 
 // In f32 the moved position i - d, formed as one number near i, keeps only
@@ -130,14 +149,25 @@ __device__ __forceinline__ void axis_at(int i, int n, float d, int &i0, float &t
 }
 
 template <>
-__device__ __forceinline__ Footprint<float> footprint_at<float>(const Dims &g, int i, int j, int k,
-                                                                float dx, float dy, float dz) {
-  int i0, j0, k0;
-  Footprint<float> f;
-  axis_at(i, g.nx, dx, i0, f.tx);
-  axis_at(j, g.ny, dy, j0, f.ty);
-  axis_at(k, g.nz, dz, k0, f.tz);
-  f.base = (k0 * g.ny + j0) * g.nx + i0;
+__device__ __forceinline__ Footprint3<float> footprint3_at<float>(const Dims &g, int i, int j,
+                                                                  int k, float dx, float dy,
+                                                                  float dz) {
+  Footprint3<float> f;
+  axis_at(i, g.nx, dx, f.i, f.tx);
+  axis_at(j, g.ny, dy, f.j, f.ty);
+  axis_at(k, g.nz, dz, f.k, f.tz);
+  return f;
+}
+
+template <typename T>
+__device__ __forceinline__ Footprint<T> footprint_at(const Dims &g, int i, int j, int k, T dx,
+                                                     T dy, T dz) {
+  const Footprint3<T> f3 = footprint3_at(g, i, j, k, dx, dy, dz);
+  Footprint<T> f;
+  f.base = f3.base(g);
+  f.tx = f3.tx;
+  f.ty = f3.ty;
+  f.tz = f3.tz;
   return f;
 }
 
@@ -177,7 +207,20 @@ struct XoshiroRng {
 };
 
 // sample_trilinear (src/fluid.rs:110-127): x-lerps, then y, then z, each as
-// a*(1-t) + b*t.
+// a*(1-t) + b*t.  lerp8 takes the 8 corner values; trilinear loads them.
+template <typename T>
+__device__ __forceinline__ T lerp8(T c000, T c100, T c010, T c110, T c001, T c101, T c011,
+                                   T c111, T tx, T ty, T tz) {
+  const T ox = T(1) - tx, oy = T(1) - ty, oz = T(1) - tz;
+  const T c00 = c000 * ox + c100 * tx;
+  const T c10 = c010 * ox + c110 * tx;
+  const T c01 = c001 * ox + c101 * tx;
+  const T c11 = c011 * ox + c111 * tx;
+  const T c0 = c00 * oy + c10 * ty;
+  const T c1 = c01 * oy + c11 * ty;
+  return c0 * oz + c1 * tz;
+}
+
 template <typename T>
 __device__ __forceinline__ T trilinear(const T *__restrict__ f, const Dims &g,
                                        const Footprint<T> &p) {
@@ -186,14 +229,7 @@ __device__ __forceinline__ T trilinear(const T *__restrict__ f, const Dims &g,
   const T c010 = __ldg(f + b + sy), c110 = __ldg(f + b + sy + sx);
   const T c001 = __ldg(f + b + sz), c101 = __ldg(f + b + sz + sx);
   const T c011 = __ldg(f + b + sz + sy), c111 = __ldg(f + b + sz + sy + sx);
-  const T ox = T(1) - p.tx, oy = T(1) - p.ty, oz = T(1) - p.tz;
-  const T c00 = c000 * ox + c100 * p.tx;
-  const T c10 = c010 * ox + c110 * p.tx;
-  const T c01 = c001 * ox + c101 * p.tx;
-  const T c11 = c011 * ox + c111 * p.tx;
-  const T c0 = c00 * oy + c10 * p.ty;
-  const T c1 = c01 * oy + c11 * p.ty;
-  return c0 * oz + c1 * p.tz;
+  return lerp8(c000, c100, c010, c110, c001, c101, c011, c111, p.tx, p.ty, p.tz);
 }
 
 // stencil_minmax (src/fluid.rs:131-150): same 8 corners, fmin/fmax keep the

@@ -3,7 +3,7 @@
 // reference's f64 arithmetic is never contracted into FMAs (rustc emits none
 // without an explicit mul_add), so the pointwise and stencil stages here
 // reproduce the reference's f64 results bit for bit.
-#include "afl_stage.cuh"
+#include "afl_stage_fused.cuh"
 
 namespace afl {
 
@@ -73,6 +73,14 @@ void launch_convert_f32_to_f64(const float *src, double *dst, int n, cudaStream_
   k_f32_to_f64<<<kReduceBlocks, kBlock, 0, st>>>(src, dst, n);
 }
 
+void launch_telemetry_finalize(const double *partials, int nparts, double time_sec,
+                               double *out8, cudaStream_t st) {
+  k_telemetry_finalize<<<1, kBlock, 0, st>>>(partials, nparts, time_sec, out8);
+}
+
+int fused_ctas(const Dims &g) { return fused_ctas_of(g); }
+
 AFL_INSTANTIATE_STAGES(double)
+AFL_INSTANTIATE_FUSED(double)
 
 }  // namespace afl

@@ -76,6 +76,37 @@ def test_advect_maccormack(af, oracle, shape, kind, precision):
     same(g, o, [name, "u", "v", "w"], precision, tol=2e-6)
 
 
+# Grids of several 32 x 8 tiles and z chunks for the fused, shared-memory
+# staged kernels: rows 16-byte aligned or not (nx a multiple of 4, even, odd),
+# and ragged tiles in x and y.
+FUSED_SHAPES = [(64, 24, 40), (70, 36, 33), (45, 17, 50)]
+
+
+@pytest.mark.parametrize("shape", FUSED_SHAPES)
+@pytest.mark.parametrize("steps_per_cell", [0.4, 3.0])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_fused_advection_tiles(af, oracle, shape, steps_per_cell, precision):
+    """The fused MacCormack kernel over many tiles and z chunks: at 0.4 cells
+    per step every footprint lies in the staged tile, at 3 cells most leave it
+    and take the global-memory path.  FP64 matches the oracle bit for bit."""
+    g, o = pair(af, oracle, shape, seed=41, vel_scale=1.0, precision=precision)
+    dt = steps_per_cell * g.h
+    for kind in range(5):
+        g.advect_maccormack_in_place(kind, dt, 0.99)
+        o.advect_maccormack_in_place(kind, dt, 0.99)
+    same(g, o, ["u", "v", "w", "density", "temperature"], precision, tol=2e-6)
+
+
+@pytest.mark.parametrize("shape", FUSED_SHAPES)
+@pytest.mark.parametrize("precision", [0, 1])
+def test_fused_forces_tiles(af, oracle, shape, precision):
+    g, o = pair(af, oracle, shape, seed=43, vel_scale=0.5, precision=precision,
+                vorticity_eps=0.3, buoyancy_beta=0.4, gravity_alpha=0.08)
+    g.apply_buoyancy_and_vorticity_confinement(0.02)
+    o.apply_buoyancy_and_vorticity_confinement(0.02)
+    same(g, o, VEL, precision, tol=1e-5)
+
+
 @pytest.mark.parametrize("shape", SHAPES)
 def test_wall_bc(af, oracle, shape):
     g, o = pair(af, oracle, shape, seed=7)
