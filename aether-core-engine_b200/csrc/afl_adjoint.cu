@@ -374,7 +374,16 @@ afl_status afl_adjoint_create(size_t nx, size_t ny, size_t nz, const afl_params 
   for (double **x : singles)
     if (st == AFL_OK) st = dalloc(a, x);
   for (int f = 0; f < 4 && st == AFL_OK; ++f) st = dalloc(a, &a->curl[f]);
-  for (int f = 0; f < 4 && st == AFL_OK; ++f) st = dalloc(a, &a->cg[f]);
+  // one block: the resident FP64 CG reads cg[0..3] as four consecutive arrays
+  if (st == AFL_OK) {
+    void *blk = nullptr;
+    if (cudaMalloc(&blk, 4 * nbytes(a)) != cudaSuccess) {
+      st = fail(AFL_ERR_OUT_OF_MEMORY, "CG vectors");
+    } else {
+      a->allocs.push_back(blk);
+      for (int f = 0; f < 4; ++f) a->cg[f] = static_cast<double *>(blk) + f * static_cast<size_t>(a->g.n);
+    }
+  }
   for (int f = 0; f < 3 && st == AFL_OK; ++f) st = dalloc(a, &a->gb[f]);
   for (int f = 0; f < 3 && st == AFL_OK; ++f) st = dalloc(a, &a->ob[f]);
   if (st != AFL_OK) return bail(st);

@@ -168,8 +168,11 @@ struct ResidentCgArgs {
   int tiles_x, tiles_y;
   double *p;            // f64 pressure
   const double *b;      // f64 right-hand side
-  void *rpub;           // published tile-edge residual (f64 or f32, n cells)
-  void *dpub0, *dpub1;  // published tile-edge direction, by iteration parity
+  void *rpub;           // mixed: published tile-edge residual (f32, n cells).
+                        // FP64: the first of four consecutive arrays of n
+                        // doubles: tile-edge r by iteration parity (0, 1), then
+                        // q = A d by parity (0, 1)
+  void *dpub0, *dpub1;  // mixed: published tile-edge direction, by iteration parity
   int max_iters;        // FP64: CG iterations; mixed: inner iterations, all passes
   int max_inner;        // mixed: inner iterations per refinement pass
   int max_refine;       // mixed: refinement passes

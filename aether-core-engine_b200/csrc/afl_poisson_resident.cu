@@ -62,7 +62,7 @@ __device__ __forceinline__ void bsum(double (&v)[NV], double *scratch) {
 // read all of sum k, and sum k+2 only after every CTA published k+1, so a
 // buffer is never rewritten while a CTA may still read it.  Tags start at 1;
 // the slots are zeroed before each launch.
-constexpr int kMaxNV = 3;
+constexpr int kMaxNV = 4;
 
 struct TagSync {
   unsigned long long *slots;  // 2 buffers x nblocks x 2*kMaxNV words
@@ -384,47 +384,127 @@ struct Halo {
 
 // Shared scratch of the reductions: per-warp values, the CTA result, and the
 // broadcast slot of the grid-wide sums.
-constexpr int kScratch = kRW * 3 + 3 + 3;
+constexpr int kScratch = kRW * kMaxNV + 2 * kMaxNV;
+constexpr int kScratchSlot = kRW * kMaxNV + kMaxNV;  // broadcast slot of the grid sums
+
+// ---- tensor memory as per-thread storage -----------------------------------
+// The FP64 kernel keeps two of its per-cell vectors in the SM's tensor memory
+// (TMEM: 128 lanes x 512 columns of 32 bits, 256 KB beside the register file
+// and shared memory).  With 1024 threads, warp w reaches lanes 32*(w%4) ..
+// +31 and owns 64 columns of them: 32 doubles per thread.  No tensor-core
+// instruction runs; 32x32b loads and stores move a thread's own columns
+// between TMEM and its registers.  The CTA allocates all 512 columns (one CTA
+// per SM) and frees them on every exit path.
+constexpr unsigned kTmCols = 512;
+
+__device__ __forceinline__ void tm_alloc_all(unsigned *dst_smem) {  // one whole warp
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(dst_smem));
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa),
+               "r"(kTmCols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tm_dealloc_all(unsigned taddr) {  // the allocating warp
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr),
+               "r"(kTmCols)
+               : "memory");
+}
+__device__ __forceinline__ void tm_sync_threads() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// 4 doubles (8 columns) of this thread's lane at column address taddr; the
+// load waits for its data inside the same statement, the store for its
+// completion, so no register is used before it is valid or reused early.
+__device__ __forceinline__ void tm_ld4(unsigned taddr, double (&v)[4]) {
+  unsigned x0, x1, x2, x3, x4, x5, x6, x7;
+  __syncwarp();  // the .sync.aligned forms need the whole warp converged
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(x0), "=r"(x1), "=r"(x2), "=r"(x3), "=r"(x4), "=r"(x5), "=r"(x6), "=r"(x7)
+      : "r"(taddr)
+      : "memory");
+  v[0] = __hiloint2double(static_cast<int>(x1), static_cast<int>(x0));
+  v[1] = __hiloint2double(static_cast<int>(x3), static_cast<int>(x2));
+  v[2] = __hiloint2double(static_cast<int>(x5), static_cast<int>(x4));
+  v[3] = __hiloint2double(static_cast<int>(x7), static_cast<int>(x6));
+}
+__device__ __forceinline__ void tm_st4(unsigned taddr, const double (&v)[4]) {
+  __syncwarp();
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};\n"
+      "tcgen05.wait::st.sync.aligned;\n" ::"r"(taddr),
+      "r"(__double2loint(v[0])), "r"(__double2hiint(v[0])), "r"(__double2loint(v[1])),
+      "r"(__double2hiint(v[1])), "r"(__double2loint(v[2])), "r"(__double2hiint(v[2])),
+      "r"(__double2loint(v[3])), "r"(__double2hiint(v[3]))
+      : "memory");
+}
 
 // ---------------------------------------------------------------- FP64 ------
 // solve_poisson_conjugate_gradient (src/fluid.rs:445-493) with the relative
-// tolerance extension.  d in shared memory, r in registers, p in global memory
-// (updated once per iteration, never read by the operator).
-// The arguments are __grid_constant__: they stay in the constant bank, which
-// leaves the compiler's 64 registers to the f64 residuals (128^3: 395 -> 413
-// Mcell-steps/s).  The mixed kernel keeps plain arguments, which measured
-// better for it.
+// tolerance extension, one grid-wide sum per iteration.
+//  * d lives in shared memory (tile + halo ring); the residual r and the
+//    pressure p live in tensor memory (TMEM); q = A d goes to global memory
+//    (L2) by iteration parity, where the neighbours also read its tile-edge
+//    values.  With r and p off the register file the kernel does not spill.
+//  * One sum carries d.q, r.q, q.q and the r.r of the current residual.
+//    alpha = delta/(d.q) takes the true delta = r.r; the next r.r, which the
+//    reference sums after r -= alpha q, is the same number expanded,
+//    delta - 2 alpha r.q + alpha^2 q.q, and gives beta = delta'/delta
+//    (src/fluid.rs:482) without a second sum.  The stopping tests after an
+//    update (:479, relative tolerance) read the true r.r, which arrives with
+//    the next iteration's sum: the test runs there, before any further update,
+//    so the iterations done and the stopping iteration are the reference's.
+//  * The halo ring of d' = (r - alpha q) + beta d is rebuilt from the
+//    neighbours' published r and q (written before the sum) with the owner's
+//    expression, bit for bit.  r edges and q are kept by iteration parity.
+//  * The stencil marches up each thread's column with the z neighbours in
+//    registers and no selects (d is exactly 0 off the interior).
+// The arguments are __grid_constant__: they stay in the constant bank.
 template <int TY, int CPT>
-__global__ void __launch_bounds__(kRT, 1)
-    k_cg_res_f64(const __grid_constant__ ResidentCgArgs a, const __grid_constant__ GridSync gs,
-                 const __grid_constant__ TagSync ts) {
+__device__ __forceinline__ void cg_f64_body(const ResidentCgArgs &a, const GridSync &gs,
+                                            const TagSync &ts, double *D, double *scratch,
+                                            double *slot, double *vals, unsigned t_r,
+                                            unsigned t_p) {
   using C = Cells<TY, CPT>;
-  extern __shared__ double Dbase[];
-  double *D = Dbase + C::SXY;  // one padding plane below plane 0
-  __shared__ double scratch[kScratch];
-  __shared__ double vals[kMaxTagBlocks * kMaxNV];
-  double *slot = scratch + kRW * 3 + 3;
+  constexpr int NCH = (CPT + 3) / 4;  // chunks of 4 doubles in TMEM
   const Dims g = a.g;
   const C cl(g, a.tiles_x);
   const Halo<TY> halo(g, a.tiles_x);
   double *p = a.p;
-  double *rpub = static_cast<double *>(a.rpub);
-  double r[CPT];
+  double *const rpub0 = static_cast<double *>(a.rpub);
+  double *const rpub1 = rpub0 + g.n;
+  double *const q0 = rpub0 + 2 * static_cast<size_t>(g.n);
+  double *const q1 = rpub0 + 3 * static_cast<size_t>(g.n);
   int phase = 0;
   {
+    // r = b - A p (src/fluid.rs:455-458) and p into TMEM, d = r.  The chunk
+    // loops stay rolled: unrolled over 16 cells they spill.
     double acc[2] = {0.0, 0.0};
+#pragma unroll 1
+    for (int ch = 0; ch < NCH; ++ch) {
+      double rv4[4] = {0.0, 0.0, 0.0, 0.0}, pv4[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int m = 0; m < CPT; ++m) {
-      r[m] = 0.0;
-      if (!cl.valid(g, m)) continue;
-      const int c = cl.c0 + m * g.nxy;
-      const double ap = cl.interior(g, m) ? lap_global(g, p, c, cl.i, cl.j, cl.k0 + m) : 0.0;
-      const double bc = __ldg(a.b + c);
-      const double rv = bc - ap;
-      r[m] = rv;
-      if (cl.edge) rpub[c] = rv;
-      acc[0] += rv * rv;
-      acc[1] += bc * bc;
+      for (int q = 0; q < 4; ++q) {
+        const int m = ch * 4 + q;
+        if (m >= CPT) break;
+        if (cl.valid(g, m)) {
+          const int c = cl.c0 + m * g.nxy;
+          const double ap = cl.interior(g, m) ? lap_global(g, p, c, cl.i, cl.j, cl.k0 + m) : 0.0;
+          const double bc = __ldg(a.b + c);
+          const double rv = bc - ap;
+          rv4[q] = rv;
+          pv4[q] = __ldcg(p + c);
+          if (cl.edge) rpub0[c] = rv;
+          acc[0] += rv * rv;
+          acc[1] += bc * bc;
+        }
+        D[cl.s0 + m * C::SXY] = rv4[q];
+      }
+      tm_st4(t_r + 8u * ch, rv4);
+      tm_st4(t_p + 8u * ch, pv4);
     }
     tag_publish<2>(ts, unsigned(phase + 1), acc, scratch);
   }
@@ -441,63 +521,115 @@ __global__ void __launch_bounds__(kRT, 1)
   const double delta0 = delta;
   double last = delta;
   int it = 0, converged = 0;
-  if (!(delta > 1e-24) || (tol2 >= 0.0 && delta <= tol2)) {
+  if (!(delta > 1e-24) || (tol2 >= 0.0 && delta <= tol2)) {  // src/fluid.rs:462
     converged = isfinite(delta) ? 1 : 0;
   } else {
-    double beta = 0.0;
-    while (it < a.max_iters) {
-      const bool first = it == 0;
-      // d = r + beta*d on the tile and its halo ring (src/fluid.rs:483-485).
-      // Cells past the grid hold r = 0, so their d stays 0: the loops below
-      // need no per-cell branches (padding planes keep every slot in bounds).
+    // the first direction on the halo ring: the neighbours' r
+    halo.fill_rolled(g, D, [&](int c, double) { return __ldcg(rpub0 + c); });
+    __syncthreads();
+    double rr_next = 0.0;
+    for (;;) {
+      const bool odd = (it & 1) != 0;
+      double *const qw = odd ? q1 : q0;
+      // q = A d (src/fluid.rs:465) marching up the column (the z neighbours in
+      // registers, the neighbour sum in the reference's order x-, x+, y-, y+,
+      // z-, z+, no selects); d.q, r.q, q.q; this residual's r.r
+      double acc[4] = {0.0, 0.0, 0.0, rr_next};
+      {
+        int s = cl.s0;
+        double below = D[s - C::SXY];
+        double mid = D[s];
+#pragma unroll 1
+        for (int ch = 0; ch < NCH; ++ch) {
+          double rc[4];
+          tm_ld4(t_r + 8u * ch, rc);
 #pragma unroll
-      for (int m = 0; m < CPT; ++m) {
-        const int s = cl.s0 + m * C::SXY;
-        D[s] = first ? r[m] : r[m] + beta * D[s];
+          for (int q = 0; q < 4; ++q) {
+            const int m = ch * 4 + q;
+            if (m >= CPT) break;
+            const double above = D[s + C::SXY];
+            const int k = cl.k0 + m;
+            const int diag = cl.diag_xy + int(k > 1) + int(k + 2 < g.nz);
+            double nb = D[s - 1];
+            nb += D[s + 1];
+            nb += D[s - C::SX];
+            nb += D[s + C::SX];
+            nb += below;
+            nb += above;
+            const double qk = cl.interior(g, m) ? double(diag) * mid - nb : 0.0;
+            acc[0] += mid * qk;
+            acc[1] += rc[q] * qk;
+            acc[2] += qk * qk;
+            if (cl.valid(g, m)) qw[cl.c0 + m * g.nxy] = qk;
+            below = mid;
+            mid = above;
+            s += C::SXY;
+          }
+        }
       }
+      tag_publish<4>(ts, unsigned(phase + 1), acc, scratch);
+      double sum[4];
+      if (!tag_gather<4>(ts, gs, unsigned(phase + 1), sum, slot, vals)) return;
+      ++phase;
+      if (it > 0) {  // the tests after the previous update (src/fluid.rs:478-481)
+        last = sum[3];
+        if (!isfinite(last)) break;
+        if (last < 1e-20) { converged = 1; break; }
+        if (tol2 >= 0.0 && last <= tol2) { converged = 1; break; }
+        delta = last;
+      }
+      if (it >= a.max_iters) break;
+      if (fabs(sum[0]) < 1e-28) break;  // src/fluid.rs:469
+      const double alpha = delta / sum[0];
+      const double dnext = delta - 2.0 * alpha * sum[1] + alpha * alpha * sum[2];
+      const double beta = dnext / delta;
+      // p += alpha d, r -= alpha q, d = r + beta d (src/fluid.rs:472-485)
+      double *const rw = odd ? rpub0 : rpub1;
+      rr_next = 0.0;
+#pragma unroll 1
+      for (int ch = 0; ch < NCH; ++ch) {
+        double rv4[4], pv4[4], qv4[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int m = ch * 4 + q;
+          qv4[q] = (m < CPT && cl.valid(g, m)) ? __ldcg(qw + cl.c0 + m * g.nxy) : 0.0;
+        }
+        tm_ld4(t_r + 8u * ch, rv4);
+        tm_ld4(t_p + 8u * ch, pv4);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int m = ch * 4 + q;
+          if (m >= CPT) continue;
+          const int s = cl.s0 + m * C::SXY;
+          const double dv = D[s];
+          pv4[q] = pv4[q] + alpha * dv;
+          const double rv = rv4[q] - alpha * qv4[q];
+          rv4[q] = rv;
+          D[s] = rv + beta * dv;
+          rr_next += rv * rv;
+          if (cl.edge && cl.valid(g, m)) rw[cl.c0 + m * g.nxy] = rv;
+        }
+        tm_st4(t_r + 8u * ch, rv4);
+        tm_st4(t_p + 8u * ch, pv4);
+      }
+      const double *const rr_ring = odd ? rpub1 : rpub0;
       halo.fill_rolled(g, D, [&](int c, double dprev) {
-        const double rv = __ldcg(rpub + c);
-        return first ? rv : rv + beta * dprev;
+        const double rv = __ldcg(rr_ring + c) - alpha * __ldcg(qw + c);
+        return rv + beta * dprev;
       });
       __syncthreads();
-      double acc[1] = {0.0};
-#pragma unroll
-      for (int m = 0; m < CPT; ++m) {
-        const int s = cl.s0 + m * C::SXY;
-        const double qv = lap_smem<double, C::SX, C::SXY>(g, D, s, cl, cl.k0 + m);
-        acc[0] += cl.interior(g, m) ? D[s] * qv : 0.0;
-      }
-      tag_publish<1>(ts, unsigned(phase + 1), acc, scratch);
-      double dq[1];
-      if (!tag_gather<1>(ts, gs, unsigned(phase + 1), dq, slot, vals)) return;
-      ++phase;
-      if (fabs(dq[0]) < 1e-28) break;  // src/fluid.rs:469
-      const double alpha = delta / dq[0];
-      double acc2[1] = {0.0};
-#pragma unroll
-      for (int m = 0; m < CPT; ++m) {
-        const int s = cl.s0 + m * C::SXY;
-        const int c = cl.c0 + m * g.nxy;
-        const double lq = lap_smem<double, C::SX, C::SXY>(g, D, s, cl, cl.k0 + m);
-        const double qv = cl.interior(g, m) ? lq : 0.0;
-        const bool v = cl.valid(g, m);
-        if (v) p[c] = p[c] + alpha * D[s];
-        const double rv = r[m] - alpha * qv;
-        r[m] = rv;
-        if (v && cl.edge) rpub[c] = rv;
-        acc2[0] += rv * rv;
-      }
-      tag_publish<1>(ts, unsigned(phase + 1), acc2, scratch);
-      double dn[1];
-      if (!tag_gather<1>(ts, gs, unsigned(phase + 1), dn, slot, vals)) return;
-      ++phase;
       ++it;
-      last = dn[0];
-      if (!isfinite(dn[0])) break;
-      if (dn[0] < 1e-20) { converged = 1; break; }  // src/fluid.rs:479
-      if (tol2 >= 0.0 && dn[0] <= tol2) { converged = 1; break; }
-      beta = dn[0] / delta;  // src/fluid.rs:482
-      delta = dn[0];
+    }
+  }
+  // the pressure back to global memory
+#pragma unroll 1
+  for (int ch = 0; ch < NCH; ++ch) {
+    double pv4[4];
+    tm_ld4(t_p + 8u * ch, pv4);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int m = ch * 4 + q;
+      if (m < CPT && cl.valid(g, m)) p[cl.c0 + m * g.nxy] = pv4[q];
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && a.report) {
@@ -511,6 +643,26 @@ __global__ void __launch_bounds__(kRT, 1)
     rep.rhs_norm = sqrt(bb);
     *a.report = rep;
   }
+}
+
+template <int TY, int CPT>
+__global__ void __launch_bounds__(kRT, 1)
+    k_cg_res_f64(const __grid_constant__ ResidentCgArgs a, const __grid_constant__ GridSync gs,
+                 const __grid_constant__ TagSync ts) {
+  using C = Cells<TY, CPT>;
+  extern __shared__ double Dbase[];
+  __shared__ double scratch[kScratch];
+  __shared__ double vals[kMaxTagBlocks * kMaxNV];
+  __shared__ unsigned tm_base;
+  const int warp = threadIdx.x >> 5;
+  if (warp == 0) tm_alloc_all(&tm_base);
+  tm_sync_threads();
+  // this thread's 64 columns: r in the first 32, p in the next 32
+  const unsigned t_r = tm_base + ((32u * unsigned(warp & 3)) << 16) + 64u * unsigned(warp >> 2);
+  cg_f64_body<TY, CPT>(a, gs, ts, Dbase + C::SXY, scratch, scratch + kScratchSlot, vals, t_r,
+                       t_r + 32u);
+  tm_sync_threads();  // every TMEM access of the CTA is complete
+  if (warp == 0) tm_dealloc_all(tm_base);
 }
 
 // ---------------------------------------------------------------- mixed -----
@@ -527,7 +679,7 @@ __global__ void __launch_bounds__(kRT, 1)
   float *Df = Dfbase + C::SXY;  // one padding plane below plane 0
   __shared__ double scratch[kScratch];
   __shared__ double vals[kMaxTagBlocks * kMaxNV];
-  double *slot = scratch + kRW * 3 + 3;
+  double *slot = scratch + kScratchSlot;
   const Dims g = a.g;
   const C cl(g, a.tiles_x);
   const Halo<TY> halo(g, a.tiles_x);
@@ -866,7 +1018,7 @@ bool plan_resident(const Dims &g, bool f64, ResidentPlan *plan) {
   if (cudaGetDevice(&dev) != cudaSuccess) return false;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const size_t static_smem = 6144;  // reduction scratch, tagged-sum values, flags, rounded up
+  const size_t static_smem = 6400;  // reduction scratch, tagged-sum values, flags, rounded up
   bool found = false;
   ResidentPlan best{};
   for (int ty : {4, 8, 16}) {
@@ -898,6 +1050,9 @@ int launch_cg_resident(const ResidentCgArgs &a, const ResidentPlan &plan, bool f
   if (!fn) return -static_cast<int>(cudaErrorInvalidConfiguration);
   const int blocks = plan.tiles_x * plan.tiles_y;
   if (blocks > ps.max_blocks) return -static_cast<int>(cudaErrorInvalidConfiguration);
+  // the tagged slots must fit the persistent state's partials (12 per CTA)
+  if (2 * 2 * kMaxNV * blocks > 12 * ps.max_blocks)
+    return -static_cast<int>(cudaErrorInvalidConfiguration);
   cudaError_t err = cudaFuncSetAttribute(reinterpret_cast<const void *>(fn),
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          plan.smem_bytes);

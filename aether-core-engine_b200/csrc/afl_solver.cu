@@ -664,7 +664,11 @@ afl_status afl_create(size_t nx, size_t ny, size_t nz, const afl_params *params,
   if (st == AFL_OK) st = alloc_as(s, &s->p, n * sizeof(double));
   if (st == AFL_OK) st = alloc_as(s, &s->b, n * sizeof(double));
   const int ncg = s->precision == AFL_PRECISION_FP64 ? 4 : 5;
-  for (int f = 0; f < ncg && st == AFL_OK; ++f) st = dev_alloc(s, &s->cg[f], fb);
+  // one block: the resident FP64 CG reads cg[0..3] as four consecutive arrays
+  void *cg_block = nullptr;
+  if (st == AFL_OK) st = dev_alloc(s, &cg_block, fb * static_cast<size_t>(ncg));
+  for (int f = 0; f < ncg && st == AFL_OK; ++f)
+    s->cg[f] = static_cast<unsigned char *>(cg_block) + fb * static_cast<size_t>(f);
   if (st == AFL_OK && s->precision == AFL_PRECISION_MIXED)
     st = alloc_as(s, &s->stage, n * sizeof(double));
   if (st == AFL_OK)
