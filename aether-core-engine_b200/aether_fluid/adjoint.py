@@ -1,8 +1,10 @@
 """Reverse mode through the FP64 smoke step (afl_adjoint_* of
 include/aether_fluid.h): controls are the initial velocity and the per-cell
 temperature amplitude of the sphere source, the output is the final density.
-`SmokeRollout` wraps one forward/backward pair with the contract of a
-torch.autograd.Function (host tensors)."""
+The step's source is the sphere, the reference's cyberpunk jets
+(inject_cyberpunk_sources, step n at time n*dt) or none; its pressure solve
+is CG or red-black SOR.  `SmokeRollout` wraps one forward/backward pair with
+the contract of a torch.autograd.Function (host tensors)."""
 from __future__ import annotations
 
 import ctypes
@@ -20,15 +22,20 @@ def _p(a):
 
 
 class Adjoint:
-    def __init__(self, nx, ny, nz, center, radius, eps=0.3, beta=0.4, alpha=0.08,
-                 cg_rel_tol=1e-10, solver_iters=2000, checkpoint_every=8, density=1.0,
-                 temperature=1.0, poisson_kernel=0):
+    SOURCES = {"cyberpunk": 0, "sphere": 1, "none": 2}
+    SOLVERS = {"cg": 0, "sor": 1}
+
+    def __init__(self, nx, ny, nz, center=(0.0, 0.0, 0.0), radius=0.0, eps=0.3, beta=0.4,
+                 alpha=0.08, cg_rel_tol=1e-10, solver_iters=2000, checkpoint_every=8,
+                 density=1.0, temperature=1.0, poisson_kernel=0, source="sphere", solver="cg",
+                 sor_omega=1.65):
         lib = _lib.load()
         self._lib = lib
         p = _lib.default_params()
         p.vorticity_eps, p.buoyancy_beta, p.gravity_alpha = eps, beta, alpha
-        p.solver_kind, p.solver_iters, p.cg_rel_tol = 0, solver_iters, cg_rel_tol
-        p.source_kind = 1
+        p.solver_kind, p.solver_iters, p.cg_rel_tol = self.SOLVERS[solver], solver_iters, cg_rel_tol
+        p.sor_omega = sor_omega
+        p.source_kind = self.SOURCES[source]
         p.poisson_kernel = poisson_kernel
         for a in range(3):
             p.sphere_center[a] = float(center[a])

@@ -2,7 +2,11 @@
 //
 // No counterpart in the reference.  Controls: the initial velocity (u, v, w)
 // and the per-cell temperature amplitude of the sphere source; output: the
-// density after `steps` steps.  The forward keeps the state every k steps.
+// density after `steps` steps.  The step's source is the sphere, the
+// reference's cyberpunk jets (inject_cyberpunk_sources at time n*dt of step
+// n; their caps are recorded) or none; its pressure solve is CG (taken as an
+// exact solve) or red-black SOR with a fixed sweep count (transposed sweep by
+// sweep; the warm start carries an adjoint from step to step).  The forward keeps the state every k steps.
 // The backward walks the segments from the last: it restores the segment's
 // checkpoint, recomputes the segment's steps recording each stage's inputs,
 // forward-sample arrays and MacCormack clamp masks (k_advect_mc_record, the
@@ -40,6 +44,13 @@ void adj_project_bwd_p(const Dims &g, double *u3b, double *v3b, double *w3b, dou
                        cudaStream_t st);
 void adj_project_bwd_b(const Dims &g, const double *u3b, const double *v3b, const double *w3b,
                        const double *bb, double *u2b, double *v2b, double *w2b, cudaStream_t st);
+void adj_jet_record(const Dims &g, double time_sec, double dt, double *rho, double *temp,
+                    double *u, double *v, double *w, unsigned char *mask, cudaStream_t st);
+void adj_jet_bwd(const Dims &g, const unsigned char *mask, double *rhob, double *tempb,
+                 cudaStream_t st);
+void adj_sor_bwd(const Dims &g, int sweeps, double omega, double *pb, double *bb,
+                 cudaStream_t st);
+void adj_add(const Dims &g, const double *x, double *y, cudaStream_t st);
 }  // namespace afl
 
 namespace {
@@ -81,6 +92,8 @@ struct Rec {
   double *u1, *v1, *w1;        // after the three velocity advections
   double *rhos, *temps;        // density/temperature after the source
   double *u3, *v3, *w3;        // after projection (advects the scalars)
+  double *u1s, *v1s, *w1s;     // jets: the velocity after the source (the curl's input)
+  unsigned char *jmask;        // jets: the caps each cell's density/temperature reached
   double *fwd[5];              // semi-Lagrangian samples of the five advections
   unsigned char *mask[5];      // MacCormack branch of every cell
 };
@@ -114,6 +127,7 @@ struct afl_adjoint {
   double *rhobs = nullptr, *tempbs = nullptr, *fb = nullptr, *pb = nullptr, *bb = nullptr;
   double *gb[3] = {}, *ob[3] = {};
   double *ampb = nullptr;
+  double *pcarry = nullptr;  // SOR: the adjoint of the next step's warm start
   int src_lo[3] = {}, src_hi[3] = {};
   float fwd_ms = 0.0f, bwd_ms = 0.0f;
   long fwd_iters = 0, adj_iters = 0;
@@ -154,7 +168,10 @@ afl_status copy(afl_adjoint *a, double *dst, const double *src) {
 // kernel when the grid fits, else the streaming one.
 afl_status solve(afl_adjoint *a, double *x, const double *rhs, long *iters) {
   int used;
-  if (a->resident) {
+  if (a->params.solver_kind == AFL_POISSON_RBSOR) {
+    afl::SorArgs sa{a->g, x, rhs, a->params.solver_iters, a->params.sor_omega, a->rep};
+    used = afl::launch_rbsor_f64(sa, a->ps, a->stream);
+  } else if (a->resident) {
     afl::ResidentCgArgs ra{};
     ra.g = a->g;
     ra.p = x;
@@ -181,20 +198,32 @@ afl_status solve(afl_adjoint *a, double *x, const double *rhs, long *iters) {
   return AFL_OK;
 }
 
-void sphere(afl_adjoint *a) {
-  afl::launch_inject_sphere<double>(a->g, a->src_lo, a->src_hi, a->F[3], a->F[4], a->amp,
-                                    a->params.sphere_center,
-                                    a->params.sphere_radius * a->params.sphere_radius,
-                                    a->params.sphere_density, a->params.sphere_temperature,
-                                    a->stream);
+bool jets(const afl_adjoint *a) { return a->params.source_kind == AFL_SOURCE_CYBERPUNK; }
+bool sphere_on(const afl_adjoint *a) { return a->params.source_kind == AFL_SOURCE_SPHERE; }
+
+// The step's source on (rho, temp, u, v, w); step n runs at time n*dt.
+void source(afl_adjoint *a, int step, double *rho, double *temp, double *u, double *v,
+            double *w) {
+  if (sphere_on(a)) {
+    afl::launch_inject_sphere<double>(a->g, a->src_lo, a->src_hi, rho, temp, a->amp,
+                                      a->params.sphere_center,
+                                      a->params.sphere_radius * a->params.sphere_radius,
+                                      a->params.sphere_density, a->params.sphere_temperature,
+                                      a->stream);
+  } else if (jets(a)) {
+    const afl::JetPair jp = afl::cyberpunk_jets(a->g, step * a->dt);
+    for (int q = 0; q < 2; ++q)
+      afl::launch_inject_jet<double>(a->g, jp.lo[q], jp.hi[q], rho, temp, u, v, w, jp.jet[q],
+                                     jp.r2, a->dt, jp.pulse, a->stream);
+  }
 }
 
-// One plain FP64 step (src/fluid.rs:598-611, sphere source), state in F/p.
-afl_status step_plain(afl_adjoint *a) {
+// One plain FP64 step (src/fluid.rs:598-611), state in F/p.
+afl_status step_plain(afl_adjoint *a, int step) {
   const afl::Dims &g = a->g;
   for (int f = 0; f < 5; ++f) {
     if (f == 3) {
-      sphere(a);
+      source(a, step, a->F[3], a->F[4], a->F[0], a->F[1], a->F[2]);
       afl::launch_curl<double>(g, a->F[0], a->F[1], a->F[2], a->curl[0], a->curl[1], a->curl[2],
                                a->curl[3], a->stream);
       afl::launch_confine_buoy<double>(g, a->F[0], a->F[1], a->F[2], a->F[3], a->F[4], a->curl[0],
@@ -217,7 +246,7 @@ afl_status step_plain(afl_adjoint *a) {
 }
 
 // The same step, keeping what its adjoint needs in R.
-afl_status step_record(afl_adjoint *a, Rec &R) {
+afl_status step_record(afl_adjoint *a, Rec &R, int step) {
   const afl::Dims &g = a->g;
   cudaStream_t st = a->stream;
   ADJ_TRY(copy(a, R.u0, a->F[0]));
@@ -237,14 +266,19 @@ afl_status step_record(afl_adjoint *a, Rec &R) {
   }
   ADJ_TRY(copy(a, R.rhos, a->F[3]));
   ADJ_TRY(copy(a, R.temps, a->F[4]));
-  afl::launch_inject_sphere<double>(g, a->src_lo, a->src_hi, R.rhos, R.temps, a->amp,
-                                    a->params.sphere_center,
-                                    a->params.sphere_radius * a->params.sphere_radius,
-                                    a->params.sphere_density, a->params.sphere_temperature, st);
   ADJ_TRY(copy(a, R.u3, R.u1));
   ADJ_TRY(copy(a, R.v3, R.v1));
   ADJ_TRY(copy(a, R.w3, R.w1));
-  afl::launch_curl<double>(g, R.u1, R.v1, R.w1, a->curl[0], a->curl[1], a->curl[2], a->curl[3], st);
+  if (jets(a)) {
+    ADJ_CUDA(cudaMemsetAsync(R.jmask, 0, static_cast<size_t>(g.n), st));
+    afl::adj_jet_record(g, step * a->dt, a->dt, R.rhos, R.temps, R.u3, R.v3, R.w3, R.jmask, st);
+    ADJ_TRY(copy(a, R.u1s, R.u3));
+    ADJ_TRY(copy(a, R.v1s, R.v3));
+    ADJ_TRY(copy(a, R.w1s, R.w3));
+  } else {
+    source(a, step, R.rhos, R.temps, R.u3, R.v3, R.w3);
+  }
+  afl::launch_curl<double>(g, R.u3, R.v3, R.w3, a->curl[0], a->curl[1], a->curl[2], a->curl[3], st);
   afl::launch_confine_buoy<double>(g, R.u3, R.v3, R.w3, R.rhos, R.temps, a->curl[0], a->curl[1],
                                    a->curl[2], a->curl[3], a->dt, a->params.vorticity_eps,
                                    a->params.buoyancy_beta, a->params.gravity_alpha, st);
@@ -279,10 +313,19 @@ afl_status step_adjoint(afl_adjoint *a, const Rec &R) {
                       a->rhob, a->fb, a->rhobs, a->ub0, a->vb0, a->wb0, st);
   // projection
   afl::adj_project_bwd_p(g, a->ub0, a->vb0, a->wb0, a->pb, st);
-  ADJ_TRY(solve(a, a->bb, a->pb, &a->adj_iters));
+  if (a->params.solver_kind == AFL_POISSON_RBSOR) {
+    // the pressure this step solved for is also the next step's warm start
+    afl::adj_add(g, a->pcarry, a->pb, st);
+    afl::adj_sor_bwd(g, a->params.solver_iters, a->params.sor_omega, a->pb, a->bb, st);
+    std::swap(a->pcarry, a->pb);
+  } else {
+    ADJ_TRY(solve(a, a->bb, a->pb, &a->adj_iters));
+  }
   afl::adj_project_bwd_b(g, a->ub0, a->vb0, a->wb0, a->bb, a->ub2, a->vb2, a->wb2, st);
-  // confinement + buoyancy (curl of u1 recomputed)
-  afl::launch_curl<double>(g, R.u1, R.v1, R.w1, a->curl[0], a->curl[1], a->curl[2], a->curl[3], st);
+  // confinement + buoyancy (curl of the velocity after the source, recomputed)
+  const double *cu = jets(a) ? R.u1s : R.u1, *cv = jets(a) ? R.v1s : R.v1,
+               *cw = jets(a) ? R.w1s : R.w1;
+  afl::launch_curl<double>(g, cu, cv, cw, a->curl[0], a->curl[1], a->curl[2], a->curl[3], st);
   ADJ_TRY(zero(a, a->ub1));
   ADJ_TRY(zero(a, a->vb1));
   ADJ_TRY(zero(a, a->wb1));
@@ -290,10 +333,14 @@ afl_status step_adjoint(afl_adjoint *a, const Rec &R) {
                        a->dt, a->params.vorticity_eps, a->params.buoyancy_beta,
                        a->params.gravity_alpha, a->gb, a->ob, a->ub1, a->vb1, a->wb1, a->rhobs,
                        a->tempbs, st);
-  // sphere source
-  afl::adj_source_bwd(g, a->src_lo, a->src_hi, a->params.sphere_center,
-                      a->params.sphere_radius * a->params.sphere_radius,
-                      a->params.sphere_temperature, a->rhobs, a->tempbs, a->ampb, st);
+  // source: the sphere's assignment, or the jets' caps (their velocity
+  // increments pass the velocity adjoint through)
+  if (sphere_on(a))
+    afl::adj_source_bwd(g, a->src_lo, a->src_hi, a->params.sphere_center,
+                        a->params.sphere_radius * a->params.sphere_radius,
+                        a->params.sphere_temperature, a->rhobs, a->tempbs, a->ampb, st);
+  else if (jets(a))
+    afl::adj_jet_bwd(g, R.jmask, a->rhobs, a->tempbs, st);
   // velocity advections, last first
   ADJ_TRY(zero(a, a->ub0));
   ADJ_TRY(zero(a, a->vb0));
@@ -332,10 +379,12 @@ afl_status afl_adjoint_create(size_t nx, size_t ny, size_t nz, const afl_params 
   *out = nullptr;
   if (nx < 6 || ny < 6 || nz < 6) return fail(AFL_ERR_INVALID_ARGUMENT, "dimensions must be >= 6");
   if (checkpoint_every < 1) return fail(AFL_ERR_INVALID_ARGUMENT, "checkpoint_every must be >= 1");
-  if (params->solver_kind != AFL_POISSON_CG)
-    return fail(AFL_ERR_INVALID_ARGUMENT, "the adjoint differentiates the CG projection only");
-  if (params->source_kind != AFL_SOURCE_SPHERE)
-    return fail(AFL_ERR_INVALID_ARGUMENT, "the adjoint needs the sphere source");
+  if (params->solver_kind != AFL_POISSON_CG && params->solver_kind != AFL_POISSON_RBSOR)
+    return fail(AFL_ERR_INVALID_ARGUMENT, "solver_kind must be 0 (CG) or 1 (RB-SOR)");
+  if (params->source_kind < AFL_SOURCE_CYBERPUNK || params->source_kind > AFL_SOURCE_NONE)
+    return fail(AFL_ERR_INVALID_ARGUMENT, "source_kind must be 0, 1 or 2");
+  if (params->solver_iters < 0)
+    return fail(AFL_ERR_INVALID_ARGUMENT, "solver_iters must be >= 0");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -370,7 +419,7 @@ afl_status afl_adjoint_create(size_t nx, size_t ny, size_t nz, const afl_params 
   double **singles[] = {&a->p, &a->b, &a->tmp_fwd, &a->tmp_out, &a->amp, &a->ub0, &a->vb0,
                         &a->wb0, &a->rhob, &a->tempb, &a->ub1, &a->vb1, &a->wb1, &a->ub2,
                         &a->vb2, &a->wb2, &a->rhobs, &a->tempbs, &a->fb, &a->pb, &a->bb,
-                        &a->ampb};
+                        &a->ampb, &a->pcarry};
   for (double **x : singles)
     if (st == AFL_OK) st = dalloc(a, x);
   for (int f = 0; f < 4 && st == AFL_OK; ++f) st = dalloc(a, &a->curl[f]);
@@ -434,6 +483,11 @@ afl_status afl_adjoint_create(size_t nx, size_t ny, size_t nz, const afl_params 
       if (st == AFL_OK) st = dalloc(a, x);
     for (int f = 0; f < 5 && st == AFL_OK; ++f) st = dalloc(a, &R.fwd[f]);
     for (int f = 0; f < 5 && st == AFL_OK; ++f) st = balloc(a, &R.mask[f]);
+    if (jets(a)) {
+      for (double **x : {&R.u1s, &R.v1s, &R.w1s})
+        if (st == AFL_OK) st = dalloc(a, x);
+      if (st == AFL_OK) st = balloc(a, &R.jmask);
+    }
   }
   if (st != AFL_OK) return bail(st);
   *out = a;
@@ -491,7 +545,7 @@ afl_status afl_adjoint_forward(afl_adjoint *a, const double *u0, const double *v
       for (int f = 0; f < 5; ++f) ADJ_TRY(copy(a, cp[f], a->F[f]));
       ADJ_TRY(copy(a, cp[5], a->p));
     }
-    ADJ_TRY(step_plain(a));
+    ADJ_TRY(step_plain(a, s));
   }
   cudaEventRecord(t1, a->stream);
   ADJ_CUDA(cudaStreamSynchronize(a->stream));
@@ -509,7 +563,8 @@ afl_status afl_adjoint_backward(afl_adjoint *a, const double *rho_bar, double *u
   if (!a->have_forward) return fail(AFL_ERR_INVALID_ARGUMENT, "run afl_adjoint_forward first");
   a->adj_iters = 0;
   ADJ_TRY(upload(a, a->rhob, rho_bar));
-  for (double *x : {a->ub0, a->vb0, a->wb0, a->tempb, a->ampb, a->bb}) ADJ_TRY(zero(a, x));
+  for (double *x : {a->ub0, a->vb0, a->wb0, a->tempb, a->ampb, a->bb, a->pcarry})
+    ADJ_TRY(zero(a, x));
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
@@ -521,7 +576,8 @@ afl_status afl_adjoint_backward(afl_adjoint *a, const double *rho_bar, double *u
     auto &cp = a->ckpt[static_cast<size_t>(seg)];
     for (int f = 0; f < 5; ++f) ADJ_TRY(copy(a, a->F[f], cp[f]));
     ADJ_TRY(copy(a, a->p, cp[5]));
-    for (int s = 0; s < count; ++s) ADJ_TRY(step_record(a, a->rec[static_cast<size_t>(s)]));
+    for (int s = 0; s < count; ++s)
+      ADJ_TRY(step_record(a, a->rec[static_cast<size_t>(s)], first + s));
     for (int s = count - 1; s >= 0; --s) ADJ_TRY(step_adjoint(a, a->rec[static_cast<size_t>(s)]));
   }
   cudaEventRecord(t1, a->stream);

@@ -386,6 +386,98 @@ __global__ void __launch_bounds__(kTx *kTy)
   w2b[c] = wall_w(g, i, j, k) ? 0.0 : wa;
 }
 
+// ---- cyberpunk jets adjoint (inject_cyberpunk_sources, src/fluid.rs:573-593) --------
+// Forward of one jet, k_inject_jet's arithmetic, recording in `mask` the cells
+// whose density (bit 2*jet) or temperature (bit 2*jet+1) reached its cap:
+// min(x, 3.8) and min(x, 4.5) pass x through below the cap and a constant at
+// or above it.  The velocity increments do not depend on the state.
+__global__ void __launch_bounds__(kTx *kTy)
+    k_jet_record(Dims g, int jet, int i0, int j0, int k0, int ni, int nj, double *rho,
+                 double *temp, double *u, double *v, double *w, double jx, double jy, double jz,
+                 double vx, double vy, double vz, double r2, double dt, double pulse,
+                 unsigned char *mask) {
+  const int ii = blockIdx.x * kTx + threadIdx.x;
+  const int jj = blockIdx.y * kTy + threadIdx.y;
+  if (ii >= ni || jj >= nj) return;
+  const int i = i0 + ii, j = j0 + jj, k = k0 + blockIdx.z;
+  const double dx = double(i) - jx;
+  const double dy = double(j) - jy;
+  const double dz = double(k) - jz;
+  const double d2 = dx * dx + dy * dy + dz * dz;
+  if (!(d2 < r2)) return;
+  const double wf = exp(-2.2 * d2 / r2);
+  const int c = (k * g.ny + j) * g.nx + i;
+  const double rn = rho[c] + dt * 9.5 * pulse * wf;
+  const double tn = temp[c] + dt * 8.2 * pulse * wf;
+  unsigned char m = mask[c];
+  if (!(rn < 3.8)) m |= static_cast<unsigned char>(1u << (2 * jet));
+  if (!(tn < 4.5)) m |= static_cast<unsigned char>(2u << (2 * jet));
+  mask[c] = m;
+  rho[c] = fmin(rn, 3.8);
+  temp[c] = fmin(tn, 4.5);
+  u[c] = u[c] + dt * vx * wf * 4.2;
+  v[c] = v[c] + dt * vy * wf * 4.2;
+  w[c] = w[c] + dt * vz * wf * 4.2;
+}
+
+// The jets' adjoint: the density/temperature adjoints pass through where no cap
+// was reached (either jet), vanish where one was; velocity adjoints pass
+// through unchanged.
+__global__ void __launch_bounds__(kBlock)
+    k_jet_bwd(int n, const unsigned char *__restrict__ mask, double *rhob, double *tempb) {
+  for (int c = blockIdx.x * kBlock + threadIdx.x; c < n; c += gridDim.x * kBlock) {
+    const unsigned m = mask[c];
+    if (m & 0x5u) rhob[c] = 0.0;
+    if (m & 0xAu) tempb[c] = 0.0;
+  }
+}
+
+// ---- red-black SOR adjoint (solve_poisson_gauss_seidel, src/fluid.rs:397-442) --------
+// A half-sweep of colour c sets, on the interior cells i of that colour,
+// p_i <- (1 - w) p_i + w (b_i + sum of p over i's interior neighbours) / diag_i,
+// a linear map of (p, b).  Its transpose: pass A lets every interior cell x of
+// the other colour gather w pb_j / diag_j from its interior neighbours j (all
+// of colour c; x is among j's neighbours exactly when both are interior), and
+// colour-c cells add w pb_i / diag_i to bb_i; pass B scales pb_i by (1 - w) on
+// colour c.  Pass A reads colour-c values only and pass B writes them only.
+__device__ __forceinline__ double sor_diag(const Dims &g, int i, int j, int k) {
+  return double(int(i > 1) + int(i + 2 < g.nx) + int(j > 1) + int(j + 2 < g.ny) + int(k > 1) +
+                int(k + 2 < g.nz));
+}
+
+__global__ void __launch_bounds__(kTx *kTy)
+    k_sor_bwd_a(Dims g, int color, double omega, double *pb, double *bb) {
+  int i, j, k;
+  if (!cell_of_thread(g, i, j, k)) return;
+  if (!interior(g, i, j, k)) return;
+  const int c = (k * g.ny + j) * g.nx + i;
+  if (((i + j + k) & 1) == color) {
+    bb[c] += omega * pb[c] / sor_diag(g, i, j, k);
+    return;
+  }
+  double acc = 0.0;
+  if (interior(g, i - 1, j, k)) acc += omega * pb[c - 1] / sor_diag(g, i - 1, j, k);
+  if (interior(g, i + 1, j, k)) acc += omega * pb[c + 1] / sor_diag(g, i + 1, j, k);
+  if (interior(g, i, j - 1, k)) acc += omega * pb[c - g.nx] / sor_diag(g, i, j - 1, k);
+  if (interior(g, i, j + 1, k)) acc += omega * pb[c + g.nx] / sor_diag(g, i, j + 1, k);
+  if (interior(g, i, j, k - 1)) acc += omega * pb[c - g.nxy] / sor_diag(g, i, j, k - 1);
+  if (interior(g, i, j, k + 1)) acc += omega * pb[c + g.nxy] / sor_diag(g, i, j, k + 1);
+  pb[c] += acc;
+}
+
+__global__ void __launch_bounds__(kTx *kTy)
+    k_sor_bwd_b(Dims g, int color, double omega, double *pb) {
+  int i, j, k;
+  if (!cell_of_thread(g, i, j, k)) return;
+  if (!interior(g, i, j, k) || ((i + j + k) & 1) != color) return;
+  const int c = (k * g.ny + j) * g.nx + i;
+  pb[c] = (1.0 - omega) * pb[c];
+}
+
+__global__ void __launch_bounds__(kBlock) k_add(int n, const double *__restrict__ x, double *y) {
+  for (int c = blockIdx.x * kBlock + threadIdx.x; c < n; c += gridDim.x * kBlock) y[c] += x[c];
+}
+
 // ---- launchers -----------------------------------------------------------------
 void adj_advect_mc_record(const Dims &g, const double *u, const double *v, const double *w,
                           const double *src, const double *fwd, double *out, double dt,
@@ -441,6 +533,44 @@ void adj_project_bwd_p(const Dims &g, double *u3b, double *v3b, double *w3b, dou
 void adj_project_bwd_b(const Dims &g, const double *u3b, const double *v3b, const double *w3b,
                        const double *bb, double *u2b, double *v2b, double *w2b, cudaStream_t st) {
   k_proj_bwd_b<<<plane_grid(g), dim3(kTx, kTy), 0, st>>>(g, u3b, v3b, w3b, bb, g.h, u2b, v2b, w2b);
+}
+
+void adj_jet_record(const Dims &g, double time_sec, double dt, double *rho, double *temp,
+                    double *u, double *v, double *w, unsigned char *mask, cudaStream_t st) {
+  const JetPair jp = cyberpunk_jets(g, time_sec);
+  for (int q = 0; q < 2; ++q) {
+    const int ni = jp.hi[q][0] - jp.lo[q][0] + 1, nj = jp.hi[q][1] - jp.lo[q][1] + 1,
+              nk = jp.hi[q][2] - jp.lo[q][2] + 1;
+    if (ni <= 0 || nj <= 0 || nk <= 0) continue;
+    dim3 grid((ni + kTx - 1) / kTx, (nj + kTy - 1) / kTy, nk);
+    const double *J = jp.jet[q];
+    k_jet_record<<<grid, dim3(kTx, kTy), 0, st>>>(g, q, jp.lo[q][0], jp.lo[q][1], jp.lo[q][2], ni,
+                                                  nj, rho, temp, u, v, w, J[0], J[1], J[2], J[3],
+                                                  J[4], J[5], jp.r2, dt, jp.pulse, mask);
+  }
+}
+
+void adj_jet_bwd(const Dims &g, const unsigned char *mask, double *rhob, double *tempb,
+                 cudaStream_t st) {
+  k_jet_bwd<<<kReduceBlocks, kBlock, 0, st>>>(g.n, mask, rhob, tempb);
+}
+
+// y += x over the grid.
+void adj_add(const Dims &g, const double *x, double *y, cudaStream_t st) {
+  k_add<<<kReduceBlocks, kBlock, 0, st>>>(g.n, x, y);
+}
+
+// (pb, bb) <- the transpose of `sweeps` red-black sweeps applied to pb: on
+// exit pb is the adjoint of the warm start and bb (zeroed here) that of the
+// right-hand side.
+void adj_sor_bwd(const Dims &g, int sweeps, double omega, double *pb, double *bb,
+                 cudaStream_t st) {
+  cudaMemsetAsync(bb, 0, sizeof(double) * static_cast<size_t>(g.n), st);
+  for (int s = sweeps - 1; s >= 0; --s)
+    for (int color = 1; color >= 0; --color) {
+      k_sor_bwd_a<<<plane_grid(g), dim3(kTx, kTy), 0, st>>>(g, color, omega, pb, bb);
+      k_sor_bwd_b<<<plane_grid(g), dim3(kTx, kTy), 0, st>>>(g, color, omega, pb);
+    }
 }
 
 }  // namespace afl

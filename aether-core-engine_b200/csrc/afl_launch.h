@@ -205,6 +205,16 @@ size_t resident_smem_bytes(const Dims &g, int ty, int cpt, bool f64);
 int launch_cg_resident(const ResidentCgArgs &a, const ResidentPlan &plan, bool f64,
                        const PersistentState &ps, cudaStream_t st);
 
+// The two orbiting jets of inject_cyberpunk_sources (src/fluid.rs:533-571) at
+// time_sec: centre and velocity of each jet, its cell box clamped as the
+// reference clamps it, the squared radius in cells and the pulse.
+struct JetPair {
+  double jet[2][6];  // centre x, y, z; velocity x, y, z
+  int lo[2][3], hi[2][3];
+  double r2, pulse;
+};
+JetPair cyberpunk_jets(const Dims &g, double time_sec);
+
 // Sets the text afl_last_error() returns on the calling thread.
 void set_last_error_text(const char *msg);
 

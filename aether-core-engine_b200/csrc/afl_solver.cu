@@ -438,37 +438,13 @@ afl_status stage_project(afl_solver *s, bool leading_bc, afl::SolveReport *rep) 
   return launch_check();
 }
 
-constexpr double kTau = 6.283185307179586;
-
 template <typename T>
 afl_status stage_inject_cyberpunk(afl_solver *s, double time_sec, double dt) {
-  // Scalars and jet geometry of src/fluid.rs:533-563, on the host.
-  const Dims &g = s->g;
-  const double cx = 0.5 * static_cast<double>(g.nx);
-  const double cz = 0.5 * static_cast<double>(g.nz);
-  const int base_j = std::min(3, g.ny - 3);
-  const double pulse = 0.65 + 0.35 * std::sin(time_sec * kTau * 0.55) +
-                       0.25 * std::fmax(std::cos(time_sec * kTau * 1.35), 0.0);
-  const double angle = time_sec * 1.85;
-  const double orbit_r = static_cast<double>(g.nx) * 0.14;
-  const double ca = std::cos(angle), sa = std::sin(angle);
-  const double jets[2][6] = {
-      {cx + orbit_r * ca, static_cast<double>(base_j) + 1.5, cz + orbit_r * sa, -2.6 * sa,
-       7.2 * pulse, 2.6 * ca},
-      {cx - orbit_r * ca, static_cast<double>(base_j) + 2.0, cz - orbit_r * sa, 2.6 * sa,
-       6.4 * pulse, -2.6 * ca},
-  };
-  const double r_cells = std::fmax(static_cast<double>(g.nx) * 0.105, 2.2);
-  const double r2 = r_cells * r_cells;
+  const afl::JetPair jp = afl::cyberpunk_jets(s->g, time_sec);
   StageTimer timer(s, AFL_STAGE_SOURCE, 2);
-  for (const auto &jet : jets) {
-    const int lo[3] = {box_lo(jet[0], r_cells, g.nx), box_lo(jet[1], r_cells, g.ny),
-                       box_lo(jet[2], r_cells, g.nz)};
-    const int hi[3] = {box_hi(jet[0], r_cells, g.nx), box_hi(jet[1], r_cells, g.ny),
-                       box_hi(jet[2], r_cells, g.nz)};
-    afl::launch_inject_jet<T>(g, lo, hi, s->F<T>(3), s->F<T>(4), s->F<T>(0), s->F<T>(1),
-                              s->F<T>(2), jet, r2, dt, pulse, s->stream);
-  }
+  for (int q = 0; q < 2; ++q)
+    afl::launch_inject_jet<T>(s->g, jp.lo[q], jp.hi[q], s->F<T>(3), s->F<T>(4), s->F<T>(0),
+                              s->F<T>(1), s->F<T>(2), jp.jet[q], jp.r2, dt, jp.pulse, s->stream);
   return launch_check();
 }
 
@@ -572,6 +548,37 @@ afl_status check_field(const afl_solver *s, int field, size_t n) {
 
 namespace afl {
 void set_last_error_text(const char *msg) { g_last_error = msg ? msg : ""; }
+
+// Scalars and jet geometry of src/fluid.rs:533-571, on the host.
+JetPair cyberpunk_jets(const Dims &g, double time_sec) {
+  constexpr double kTau = 6.283185307179586;
+  const double cx = 0.5 * static_cast<double>(g.nx);
+  const double cz = 0.5 * static_cast<double>(g.nz);
+  const int base_j = std::min(3, g.ny - 3);
+  JetPair jp{};
+  jp.pulse = 0.65 + 0.35 * std::sin(time_sec * kTau * 0.55) +
+             0.25 * std::fmax(std::cos(time_sec * kTau * 1.35), 0.0);
+  const double angle = time_sec * 1.85;
+  const double orbit_r = static_cast<double>(g.nx) * 0.14;
+  const double ca = std::cos(angle), sa = std::sin(angle);
+  const double jets[2][6] = {
+      {cx + orbit_r * ca, static_cast<double>(base_j) + 1.5, cz + orbit_r * sa, -2.6 * sa,
+       7.2 * jp.pulse, 2.6 * ca},
+      {cx - orbit_r * ca, static_cast<double>(base_j) + 2.0, cz - orbit_r * sa, 2.6 * sa,
+       6.4 * jp.pulse, -2.6 * ca},
+  };
+  const double r_cells = std::fmax(static_cast<double>(g.nx) * 0.105, 2.2);
+  jp.r2 = r_cells * r_cells;
+  const int n[3] = {g.nx, g.ny, g.nz};
+  for (int q = 0; q < 2; ++q) {
+    for (int a = 0; a < 6; ++a) jp.jet[q][a] = jets[q][a];
+    for (int a = 0; a < 3; ++a) {
+      jp.lo[q][a] = box_lo(jets[q][a], r_cells, n[a]);
+      jp.hi[q][a] = box_hi(jets[q][a], r_cells, n[a]);
+    }
+  }
+  return jp;
+}
 }  // namespace afl
 
 // ============================================================================

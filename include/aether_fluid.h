@@ -303,13 +303,19 @@ afl_status afl_rng_f64(uint64_t seed, uint64_t skip, size_t n, double *out);
 /* ---- reverse mode (no reference counterpart) --------------------------------
  * Gradient of a function of the final density with respect to the initial
  * velocity and the per-cell temperature amplitude of the sphere source, through
- * `steps` FP64 steps (sphere source, CG projection).  Hand-written adjoints of
- * every stage; MacCormack clamp branches are recorded; the adjoint pressure
- * solve uses the same symmetric-operator CG (solves treated as exact, so use a
- * tight cg_rel_tol).  The state is checkpointed every `checkpoint_every` steps
- * and each segment is recomputed during the backward pass. */
+ * `steps` FP64 steps.  Hand-written adjoints of every stage; MacCormack clamp
+ * branches and the jets' caps are recorded.  Sources: the sphere
+ * (AFL_SOURCE_SPHERE), the reference's cyberpunk jets (step n at time n*dt)
+ * or none.  Pressure solves: CG, whose adjoint solve uses the same
+ * symmetric-operator CG (solves treated as exact, so use a tight cg_rel_tol),
+ * or red-black SOR with solver_iters sweeps, transposed sweep by sweep (its
+ * warm start from the previous step's pressure carries an adjoint between
+ * steps).  The state is checkpointed every `checkpoint_every` steps and each
+ * segment is recomputed during the backward pass.  FP64 only
+ * (params.precision is ignored). */
 typedef struct afl_adjoint afl_adjoint;
-/* params: source_kind must be AFL_SOURCE_SPHERE, solver_kind AFL_POISSON_CG. */
+/* params: source_kind and solver_kind as above; poisson_kernel picks the CG
+ * kernel as in afl_create. */
 afl_status afl_adjoint_create(size_t nx, size_t ny, size_t nz, const afl_params *params,
                               int checkpoint_every, afl_adjoint **out);
 afl_status afl_adjoint_destroy(afl_adjoint *a);

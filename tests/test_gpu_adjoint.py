@@ -207,3 +207,122 @@ def test_torch_autograd_function(af, case):
     L.backward()
     for t, ref in zip(x, case["grads"]):
         assert rel_l2(t.grad.numpy(), ref) <= 1e-9
+
+
+# ---- the reference's jet source and the red-black SOR projection --------------
+def oracle_rollout(O, shape, x, steps, dt, source_kind, solver, iters, omega=1.65,
+                   center=None, radius=None):
+    """The f64 CPU oracle from initial velocity x[:3] (amplitude x[3] for the
+    sphere): the final density."""
+    s = O.OracleSolver(*shape)
+    s.set_params(vorticity_eps=0.3, buoyancy_beta=0.4, gravity_alpha=0.08,
+                 solver_kind=O.CG if solver == "cg" else O.RBGS, solver_iters=iters,
+                 cg_rel_tol=CG_REL_TOL if solver == "cg" else 0.0, sor_omega=omega)
+    for name, arr in zip(("u", "v", "w"), x[:3]):
+        s.field(name)[:] = arr
+    if source_kind == "sphere":
+        s.set_sphere_source(center, radius, 1.0, 1.0, temp_amp=x[3])
+    else:
+        s.set_source_kind(O.SOURCE_CYBERPUNK)
+    for n in range(steps):
+        s.step(dt, n * dt)
+    return s.field("density").copy()
+
+
+@pytest.mark.parametrize("source_kind,solver", [("cyberpunk", "cg"), ("sphere", "sor"),
+                                                ("cyberpunk", "sor")])
+def test_jet_and_sor_adjoints(af, oracle, source_kind, solver):
+    """The adjoint through the reference's own source (inject_cyberpunk_sources,
+    src/fluid.rs:532-595) and through the red-black SOR projection
+    (src/fluid.rs:397-442): the forward equals the oracle's, and the gradient
+    agrees with central differences of the GPU forward (3 directions) and of
+    the oracle (1 direction).  The jets run at 1.5 cells per step."""
+    from aether_fluid.adjoint import Adjoint
+    u, v, w, amp = controls(SHAPE, 5)
+    dt = (1.5 if source_kind == "cyberpunk" else 0.5) / max(SHAPE)
+    center, radius = (SHAPE[0] / 2, 0.1 * SHAPE[1] + 1.0, SHAPE[2] / 2), 3.0
+    iters = CG_ITERS if solver == "cg" else 30
+    adj = Adjoint(*SHAPE, source=source_kind, solver=solver, checkpoint_every=4,
+                  cg_rel_tol=CG_REL_TOL, solver_iters=iters, sor_omega=1.7, center=center,
+                  radius=radius)
+    x = (u, v, w, amp)
+    tu, tv, tw, _ = controls(SHAPE, 6)
+    tgt = adj.forward(tu, tv, tw, amp, STEPS, dt)
+    rho = adj.forward(*x, STEPS, dt)
+    ref = oracle_rollout(oracle, SHAPE, x, STEPS, dt, source_kind, solver, iters, 1.7, center,
+                         radius)
+    assert rel_l2(rho, ref) <= 1e-9
+    g = adj.backward(rho - tgt)
+    if source_kind == "cyberpunk":
+        assert not np.any(g[3])           # the jets have no amplitude control
+    gnorm = np.sqrt(sum(float(np.dot(a, a)) for a in g))
+    assert gnorm > 0
+
+    def loss_gpu(xx):
+        return 0.5 * float(np.sum((adj.forward(*xx, STEPS, dt) - tgt) ** 2))
+
+    def loss_oracle(xx):
+        return 0.5 * float(np.sum((oracle_rollout(oracle, SHAPE, xx, STEPS, dt, source_kind,
+                                                  solver, iters, 1.7, center, radius)
+                                   - tgt) ** 2))
+
+    for n, d in enumerate(directions(x[0].size, 4, 37)):
+        if source_kind == "cyberpunk":
+            d[3] = np.zeros_like(d[3])
+        ad = sum(float(np.dot(a, b)) for a, b in zip(g, d))
+        fd = central(loss_gpu if n < 3 else loss_oracle, x, d, EPS)
+        assert abs(fd - ad) <= 1e-3 * max(abs(ad), 1e-3 * gnorm), (n, fd, ad)
+    adj.close()
+
+
+def test_adjoint_c4_reduced_against_oracle_fd(af, oracle):
+    """The adjoint workload at reduced size: 32^3, 16 steps, a checkpoint every
+    8; controls are the initial velocity (seed-0 noise in [-0.01, 0.01], wall
+    BC) and the sphere's temperature amplitude (seed 2, uniform in [0.5, 1.5]);
+    L = 0.5*|rho - rho_target|^2, the target's source 3 cells further in x;
+    pressure solves to 1e-12.  The adjoint's directional derivative along 4
+    seeded directions agrees with central differences (eps 1e-7) of the f64
+    CPU oracle to 1e-3."""
+    from aether_fluid.adjoint import Adjoint
+    from aether_fluid.ensemble import rng_f64
+    n, steps = 32, 16
+    cells = n ** 3
+    dt = 0.5 / n
+    center, radius = (n / 2, 0.1 * n, n / 2), 5.0 * n / 64.0
+    noise = rng_f64(0, 0, 3 * cells)
+
+    def make_c4(cx):
+        return Adjoint(n, n, n, center=(cx, center[1], center[2]), radius=radius,
+                       checkpoint_every=8, cg_rel_tol=1e-12, solver_iters=4000)
+
+    adj = make_c4(center[0])
+    u, v, w = adj.wall_masked(*(-0.01 + 0.02 * noise[a * cells:(a + 1) * cells]
+                                for a in range(3)))
+    x = (u, v, w, 0.5 + rng_f64(2, 0, cells))
+    t = make_c4(center[0] + 3.0)
+    tgt = t.forward(*x, steps, dt)
+    t.close()
+    rho = adj.forward(*x, steps, dt)
+    g = adj.backward(rho - tgt)
+
+    def loss_oracle(xx):
+        s = oracle.OracleSolver(n, n, n)
+        s.set_params(vorticity_eps=0.3, buoyancy_beta=0.4, gravity_alpha=0.08,
+                     solver_kind=oracle.CG, solver_iters=4000, cg_rel_tol=1e-12)
+        for name, arr in zip(("u", "v", "w"), xx[:3]):
+            s.field(name)[:] = arr
+        s.set_sphere_source(center, radius, 1.0, 1.0, temp_amp=xx[3])
+        for k in range(steps):
+            s.step(dt, k * dt)
+        return 0.5 * float(np.sum((s.field("density") - tgt) ** 2))
+
+    rng = np.random.default_rng(11)
+    for _ in range(4):
+        d = [rng.standard_normal(cells) for _ in range(4)]
+        d[0], d[1], d[2] = adj.wall_masked(d[0], d[1], d[2])
+        nrm = np.sqrt(sum(float(np.dot(a, a)) for a in d))
+        d = [a / nrm for a in d]
+        ad = sum(float(np.dot(a, b)) for a, b in zip(g, d))
+        fd = central(loss_oracle, x, d, 1e-7)
+        assert abs(fd - ad) <= 1e-3 * abs(ad), (fd, ad)
+    adj.close()

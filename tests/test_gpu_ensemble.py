@@ -54,6 +54,37 @@ def test_ensemble_matches_single_solvers(af, precision, tol):
         assert all(abs(a - b) <= 1 for a, b in zip(its, its1)), (m, its, its1)
 
 
+@pytest.mark.parametrize("precision,tol", [(0, 1e-8), (1, 1e-4)])
+def test_ensemble_matches_oracle(af, oracle, precision, tol):
+    """Every instance of a batched ensemble of four grid sizes against its own
+    run of the f64 CPU oracle (src/fluid.rs:598-611 with the sphere source):
+    the fields after 5 steps within 1e-8 relative L2 (FP64; the batched CG
+    sums in another order) or 1e-4 (mixed), and, in FP64, the per-step CG
+    iteration counts within 1."""
+    from aether_fluid.ensemble import Ensemble
+    O = oracle
+    specs = specs_small()
+    steps = 5
+    ens = Ensemble(specs, precision=precision)
+    tel, infos = ens.run(steps)
+    for m, spec in enumerate(specs):
+        o = O.OracleSolver(spec.nx, spec.ny, spec.nz)
+        o.set_params(vorticity_eps=spec.eps, buoyancy_beta=spec.beta, gravity_alpha=spec.alpha,
+                     solver_kind=O.CG, solver_iters=200, cg_rel_tol=1e-6)
+        o.init_velocity_noise(spec.seed, -spec.noise, spec.noise)
+        o.set_sphere_source(spec.center, spec.radius)
+        its = []
+        for n in range(steps):
+            o.step(spec.dt, n * spec.dt)
+            its.append(o.last_cg_iters())
+        for f in ("u", "v", "w", "density", "temperature"):
+            err = rel_l2(ens.field(m, f), o.field(f))
+            assert err <= tol, (m, f, err)
+        if precision == 0:
+            got = [infos[n][m].iterations for n in range(steps)]
+            assert all(abs(a - b) <= 1 for a, b in zip(got, its)), (m, got, its)
+
+
 def test_ensemble_autotune_restores_state(af):
     from aether_fluid.ensemble import Ensemble
     specs = specs_small()
