@@ -558,6 +558,33 @@ def cpu_model() -> str:
     return "unknown"
 
 
+def summary(variants, large, ensemble, adjoint) -> dict:
+    """The figures a reader looks for first, in a few short keys at the end of
+    the line (the full sections come before it)."""
+    r3 = lambda x: round(x, 3) if isinstance(x, (int, float)) else x  # noqa: E731
+    out = {f"{k}_mcells": r3(v["value"]) for k, v in variants.items()}
+    if "mixed_cg" in variants and "fp64_cg" in variants:
+        out["mixed_over_fp64_128"] = r3(variants["mixed_cg"]["speedup_vs_fp64_cg"])
+        out["mixed_rel_l2_vs_fp64"] = {f: float(f"{e:.2e}") for f, e in
+                                       variants["mixed_cg"]["rel_l2_vs_fp64_cg"].items()}
+    if large and "mixed_cg" in large:
+        out["large_256"] = {
+            "mixed_mcells": r3(large["mixed_cg"]["value"]),
+            "fp64_mcells": r3(large["fp64_cg"]["value"]),
+            "mixed_over_fp64": r3(large["mixed_over_fp64"]),
+            "stage_frac_fp64": {k: r3(v) for k, v in
+                                large["fp64_cg"]["stage_roofline_frac"].items()},
+            "stage_frac_mixed": {k: r3(v) for k, v in
+                                 large["mixed_cg"]["stage_roofline_frac"].items()}}
+    if ensemble and "speedup" in ensemble:
+        out["ensemble_mcells"] = r3(ensemble["batched_mcell_steps_per_s"])
+        out["ensemble_speedup"] = r3(ensemble["speedup"])
+    if adjoint and "adjoint_fwd_ratio" in adjoint:
+        out["adjoint_fwd_ratio"] = r3(adjoint["adjoint_fwd_ratio"])
+        out["adjoint_fd_eps1e-7_max"] = adjoint["fd"].get("eps_1e-07", {}).get("rel_err_max")
+    return out
+
+
 def run_ours(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -722,6 +749,7 @@ def run_ours(args):
                            f"(CG iters {cpu['cg_iters']}), {cpu['seconds']:.1f} s on "
                            f"{cpu_model()}")}
         line["clocks"] = clocks
+        line["summary"] = summary(variants, large, ensemble, adjoint)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
