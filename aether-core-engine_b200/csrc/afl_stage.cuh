@@ -269,6 +269,58 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
+// The same stage on runs of 4 cells along x (grids with nx % 4 == 0): each
+// thread loads its run of u, v, w as vectors plus the one u value past it,
+// with the per-cell arithmetic of k_divergence.  A fixed grid of
+// kReduceBlocks CTAs walks the runs, so the sums stay reproducible.
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    k_divergence_x4(Dims g, const T *__restrict__ u, const T *__restrict__ v,
+                    const T *__restrict__ w, double *__restrict__ b,
+                    double *__restrict__ partials, double inv_h, double h) {
+  __shared__ double scratch[kWarps * 2];
+  double acc[2] = {0.0, 0.0};
+  const int runs = g.n / 4, rx = g.nx / 4;
+  for (int r = blockIdx.x * kBlock + threadIdx.x; r < runs; r += gridDim.x * kBlock) {
+    const int row = r / rx;
+    const int i0 = (r - row * rx) * 4;
+    const int k = row / g.ny, j = row - k * g.ny;
+    const int c = row * g.nx + i0;
+    double bv[4] = {0.0, 0.0, 0.0, 0.0};
+    if (j >= 1 && j <= g.ny - 2 && k >= 1 && k <= g.nz - 2) {
+      T uu[5], vc[4], vn[4], wc[4], wn[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        uu[a] = u[c + a];
+        vc[a] = v[c + a];
+        vn[a] = v[c + g.nx + a];
+        wc[a] = w[c + a];
+        wn[a] = w[c + g.nxy + a];
+      }
+      uu[4] = i0 + 4 < g.nx ? u[c + 4] : T(0);
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int i = i0 + a;
+        if (i < 1 || i > g.nx - 2) continue;
+        const double du = double(uu[a + 1]) - double(uu[a]);
+        const double dv = double(vn[a]) - double(vc[a]);
+        const double dw = double(wn[a]) - double(wc[a]);
+        const double div_val = (du + dv + dw) * inv_h;
+        bv[a] = -h * (du + dv + dw);
+        acc[0] += div_val * div_val;
+        acc[1] += bv[a] * bv[a];
+      }
+    }
+    reinterpret_cast<double2 *>(b + c)[0] = make_double2(bv[0], bv[1]);
+    reinterpret_cast<double2 *>(b + c)[1] = make_double2(bv[2], bv[3]);
+  }
+  block_sum<2>(acc, scratch);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x * 2 + 0] = acc[0];
+    partials[blockIdx.x * 2 + 1] = acc[1];
+  }
+}
+
 // Finishes k_divergence: out2 = {RMS divergence, ||b||_2}.
 __global__ void __launch_bounds__(kBlock)
     k_divergence_finalize(const double *__restrict__ partials, int nparts,
@@ -302,6 +354,57 @@ __global__ void __launch_bounds__(kTx *kTy)
   for_column_cells(g, [&](int i, int j, int k) {
     cell_project(g, u, v, w, p, inv_h, i, j, k);
   });
+}
+
+// The same stage on runs of 4 cells along x (nx % 4 == 0), one run per
+// thread, with cell_project's arithmetic: the run's u, v, w and the pressure
+// values it needs are all loaded before any is used.
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    k_project_x4(Dims g, T *__restrict__ u, T *__restrict__ v, T *__restrict__ w,
+                 const double *__restrict__ p, double inv_h) {
+  const int runs = g.n / 4, rx = g.nx / 4;
+  const int r = blockIdx.x * kBlock + threadIdx.x;
+  if (r >= runs) return;
+  const int row = r / rx;
+  const int i0 = (r - row * rx) * 4;
+  const int k = row / g.ny, j = row - k * g.ny;
+  const int c = row * g.nx + i0;
+  T uu[4], vv[4], ww[4];
+  double pc[4], pxm[4], pym[4], pzm[4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    uu[a] = u[c + a];
+    vv[a] = v[c + a];
+    ww[a] = w[c + a];
+  }
+  const bool rin = j >= 1 && j <= g.ny - 2 && k >= 1 && k <= g.nz - 2;
+  if (rin) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      pc[a] = p[c + a];
+      pym[a] = p[c - g.nx + a];
+      pzm[a] = p[c - g.nxy + a];
+    }
+    pxm[0] = i0 > 0 ? p[c - 1] : 0.0;
+#pragma unroll
+    for (int a = 1; a < 4; ++a) pxm[a] = pc[a - 1];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int i = i0 + a;
+      if (i < 1 || i > g.nx - 2) continue;
+      if (i > 1) uu[a] = T(double(uu[a]) - (pc[a] - pxm[a]) * inv_h);
+      if (j > 1) vv[a] = T(double(vv[a]) - (pc[a] - pym[a]) * inv_h);
+      if (k > 1) ww[a] = T(double(ww[a]) - (pc[a] - pzm[a]) * inv_h);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int i = i0 + a;
+    u[c + a] = wall_u(g, i, j, k) ? T(0) : uu[a];
+    v[c + a] = wall_v(g, i, j, k) ? T(0) : vv[a];
+    w[c + a] = wall_w(g, i, j, k) ? T(0) : ww[a];
+  }
 }
 
 // ---- sources -----------------------------------------------------------------
@@ -484,14 +587,20 @@ template <typename T>
 void launch_divergence(const Dims &g, const T *u, const T *v, const T *w, double *b,
                        double *partials, double *out2, cudaStream_t st) {
   const double inv_h = 1.0 / g.h;
-  k_divergence<T><<<kReduceBlocks, kBlock, 0, st>>>(g, u, v, w, b, partials, inv_h, g.h);
+  if (g.nx % 4 == 0)
+    k_divergence_x4<T><<<kReduceBlocks, kBlock, 0, st>>>(g, u, v, w, b, partials, inv_h, g.h);
+  else
+    k_divergence<T><<<kReduceBlocks, kBlock, 0, st>>>(g, u, v, w, b, partials, inv_h, g.h);
   const double interior_cells = double(g.nx - 2) * double(g.ny - 2) * double(g.nz - 2);
   k_divergence_finalize<<<1, kBlock, 0, st>>>(partials, kReduceBlocks, interior_cells, out2);
 }
 
 template <typename T>
 void launch_project(const Dims &g, T *u, T *v, T *w, const double *p, cudaStream_t st) {
-  k_project<T><<<column_grid(g), dim3(kTx, kTy), 0, st>>>(g, u, v, w, p, 1.0 / g.h);
+  if (g.nx % 4 == 0)
+    k_project_x4<T><<<(g.n / 4 + kBlock - 1) / kBlock, kBlock, 0, st>>>(g, u, v, w, p, 1.0 / g.h);
+  else
+    k_project<T><<<column_grid(g), dim3(kTx, kTy), 0, st>>>(g, u, v, w, p, 1.0 / g.h);
 }
 
 template <typename T>

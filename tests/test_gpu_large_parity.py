@@ -71,6 +71,7 @@ def gpu_run(af, plume_name, precision, steps):
 
 def check(fields, ref, precision):
     errs = {f: rel_l2(fields[f], ref[f]) for f in FIELDS}
+    print("relative L2 against the oracle:", {f: f"{e:.2e}" for f, e in errs.items()})
     for f, e in errs.items():
         assert e <= TOL[precision], (f, errs)
     return errs
