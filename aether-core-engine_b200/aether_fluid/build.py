@@ -24,8 +24,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
           "--expt-relaxed-constexpr", "-extended-lambda"]
 # Units whose f64 arithmetic must not be contracted into FMAs.
 NO_FMA = {"afl_kernels_f64.cu", "afl_poisson_f64.cu", "afl_poisson_resident.cu",
-          "afl_poisson_stream.cu", "afl_poisson_onepass.cu", "afl_ensemble_f64.cu",
-          "afl_adjoint_kernels.cu",
+          "afl_poisson_stream.cu", "afl_ensemble_f64.cu", "afl_adjoint_kernels.cu",
           "afl_medium.cu"}
 SOURCES = [
     "afl_kernels_f64.cu",
@@ -34,7 +33,6 @@ SOURCES = [
     "afl_poisson_mixed.cu",
     "afl_poisson_resident.cu",
     "afl_poisson_stream.cu",
-    "afl_poisson_onepass.cu",
     "afl_solver.cu",
     "afl_noalloc.cu",
     "afl_ensemble_f64.cu",

@@ -142,10 +142,6 @@ struct MixedCgArgs {
   SolveReport *report;
 };
 int launch_cg_mixed(const MixedCgArgs &a, const PersistentState &ps, cudaStream_t st);
-// The same solve at one pass over the grid per iteration (afl_poisson_onepass.cu):
-// r and d alternate between (r, q) and (d0, d1) by pass parity.
-int launch_cg_onepass_mixed(const MixedCgArgs &a, const PersistentState &ps, cudaStream_t st);
-int persistent_blocks_onepass();
 
 struct SorMixedArgs {
   Dims g;

@@ -97,9 +97,8 @@ int persistent_blocks_sor_mixed() {
   return blocks_for(reinterpret_cast<const void *>(&k_rbsor_mixed));
 }
 
-// The single-grid mixed CG that streams through HBM: one pass per iteration.
 int launch_cg_mixed(const MixedCgArgs &a, const PersistentState &ps, cudaStream_t st) {
-  return launch_cg_onepass_mixed(a, ps, st);
+  return launch_cg_stream_mixed(a, ps, st);
 }
 
 int launch_rbsor_mixed(const SorMixedArgs &a, const PersistentState &ps, cudaStream_t st) {

@@ -688,7 +688,6 @@ afl_status afl_create(size_t nx, size_t ny, size_t nz, const afl_params *params,
   int maxb = std::max(std::max(afl::persistent_blocks_cg_f64(), afl::persistent_blocks_sor_f64()),
                       std::max(afl::persistent_blocks_cg_mixed(),
                                afl::persistent_blocks_sor_mixed()));
-  maxb = std::max(maxb, afl::persistent_blocks_onepass());
   s->ps.max_blocks = maxb;
   s->resident_ok = afl::plan_resident(s->g, s->precision == AFL_PRECISION_FP64, &s->resident);
   s->ps.timeout_ns = 5000000000ull;  // 5 s per barrier wait

@@ -269,10 +269,12 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// The same stage on runs of 4 cells along x (grids with nx % 4 == 0): each
-// thread loads its run of u, v, w as vectors plus the one u value past it,
-// with the per-cell arithmetic of k_divergence.  A fixed grid of
-// kReduceBlocks CTAs walks the runs, so the sums stay reproducible.
+// The same stage with four cells per thread (grids with nx % 128 == 0): a
+// warp covers 128 consecutive cells of a row and lane l takes cells l, l+32,
+// l+64 and l+96, so every load and store is coalesced and each thread has
+// four cells' loads in flight; the per-cell arithmetic is k_divergence's.  A
+// fixed grid of kReduceBlocks CTAs walks the rows, so the sums stay
+// reproducible.
 template <typename T>
 __global__ void __launch_bounds__(kBlock)
     k_divergence_x4(Dims g, const T *__restrict__ u, const T *__restrict__ v,
@@ -280,29 +282,34 @@ __global__ void __launch_bounds__(kBlock)
                     double *__restrict__ partials, double inv_h, double h) {
   __shared__ double scratch[kWarps * 2];
   double acc[2] = {0.0, 0.0};
-  const int runs = g.n / 4, rx = g.nx / 4;
-  for (int r = blockIdx.x * kBlock + threadIdx.x; r < runs; r += gridDim.x * kBlock) {
-    const int row = r / rx;
-    const int i0 = (r - row * rx) * 4;
+  const int lane = threadIdx.x & 31;
+  const int segs = g.n / 128, sx = g.nx / 128;
+  for (int sgi = (blockIdx.x * kBlock + threadIdx.x) / 32; sgi < segs;
+       sgi += gridDim.x * kWarps) {
+    const int row = sgi / sx;
+    const int i0 = (sgi - row * sx) * 128 + lane;
     const int k = row / g.ny, j = row - k * g.ny;
-    const int c = row * g.nx + i0;
+    const int c0 = row * g.nx + i0;
+    const bool rin = j >= 1 && j <= g.ny - 2 && k >= 1 && k <= g.nz - 2;
     double bv[4] = {0.0, 0.0, 0.0, 0.0};
-    if (j >= 1 && j <= g.ny - 2 && k >= 1 && k <= g.nz - 2) {
-      T uu[5], vc[4], vn[4], wc[4], wn[4];
+    if (rin) {
+      T uc[4], un[4], vc[4], vn[4], wc[4], wn[4];
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
-        uu[a] = u[c + a];
-        vc[a] = v[c + a];
-        vn[a] = v[c + g.nx + a];
-        wc[a] = w[c + a];
-        wn[a] = w[c + g.nxy + a];
+        const int c = c0 + 32 * a;
+        const bool in_x = i0 + 32 * a + 1 < g.nx;
+        uc[a] = u[c];
+        un[a] = in_x ? u[c + 1] : T(0);
+        vc[a] = v[c];
+        vn[a] = v[c + g.nx];
+        wc[a] = w[c];
+        wn[a] = w[c + g.nxy];
       }
-      uu[4] = i0 + 4 < g.nx ? u[c + 4] : T(0);
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
-        const int i = i0 + a;
+        const int i = i0 + 32 * a;
         if (i < 1 || i > g.nx - 2) continue;
-        const double du = double(uu[a + 1]) - double(uu[a]);
+        const double du = double(un[a]) - double(uc[a]);
         const double dv = double(vn[a]) - double(vc[a]);
         const double dw = double(wn[a]) - double(wc[a]);
         const double div_val = (du + dv + dw) * inv_h;
@@ -311,8 +318,8 @@ __global__ void __launch_bounds__(kBlock)
         acc[1] += bv[a] * bv[a];
       }
     }
-    reinterpret_cast<double2 *>(b + c)[0] = make_double2(bv[0], bv[1]);
-    reinterpret_cast<double2 *>(b + c)[1] = make_double2(bv[2], bv[3]);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) b[c0 + 32 * a] = bv[a];
   }
   block_sum<2>(acc, scratch);
   if (threadIdx.x == 0) {
@@ -356,54 +363,49 @@ __global__ void __launch_bounds__(kTx *kTy)
   });
 }
 
-// The same stage on runs of 4 cells along x (nx % 4 == 0), one run per
-// thread, with cell_project's arithmetic: the run's u, v, w and the pressure
-// values it needs are all loaded before any is used.
+// The same stage with four cells per thread (nx % 128 == 0): a warp covers
+// 128 consecutive cells of a row, lane l takes cells l, l+32, l+64 and
+// l+96, so every load and store is coalesced; cell_project's arithmetic.
 template <typename T>
 __global__ void __launch_bounds__(kBlock)
     k_project_x4(Dims g, T *__restrict__ u, T *__restrict__ v, T *__restrict__ w,
                  const double *__restrict__ p, double inv_h) {
-  const int runs = g.n / 4, rx = g.nx / 4;
-  const int r = blockIdx.x * kBlock + threadIdx.x;
-  if (r >= runs) return;
-  const int row = r / rx;
-  const int i0 = (r - row * rx) * 4;
+  const int lane = threadIdx.x & 31;
+  const int sgi = (blockIdx.x * kBlock + threadIdx.x) / 32;
+  if (sgi >= g.n / 128) return;
+  const int sx = g.nx / 128;
+  const int row = sgi / sx;
+  const int i0 = (sgi - row * sx) * 128 + lane;
   const int k = row / g.ny, j = row - k * g.ny;
-  const int c = row * g.nx + i0;
+  const int c0 = row * g.nx + i0;
+  const bool rin = j >= 1 && j <= g.ny - 2 && k >= 1 && k <= g.nz - 2;
   T uu[4], vv[4], ww[4];
   double pc[4], pxm[4], pym[4], pzm[4];
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
-    uu[a] = u[c + a];
-    vv[a] = v[c + a];
-    ww[a] = w[c + a];
-  }
-  const bool rin = j >= 1 && j <= g.ny - 2 && k >= 1 && k <= g.nz - 2;
-  if (rin) {
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      pc[a] = p[c + a];
-      pym[a] = p[c - g.nx + a];
-      pzm[a] = p[c - g.nxy + a];
-    }
-    pxm[0] = i0 > 0 ? p[c - 1] : 0.0;
-#pragma unroll
-    for (int a = 1; a < 4; ++a) pxm[a] = pc[a - 1];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const int i = i0 + a;
-      if (i < 1 || i > g.nx - 2) continue;
-      if (i > 1) uu[a] = T(double(uu[a]) - (pc[a] - pxm[a]) * inv_h);
-      if (j > 1) vv[a] = T(double(vv[a]) - (pc[a] - pym[a]) * inv_h);
-      if (k > 1) ww[a] = T(double(ww[a]) - (pc[a] - pzm[a]) * inv_h);
+    const int c = c0 + 32 * a;
+    uu[a] = u[c];
+    vv[a] = v[c];
+    ww[a] = w[c];
+    if (rin) {
+      pc[a] = p[c];
+      pxm[a] = i0 + 32 * a > 0 ? p[c - 1] : 0.0;
+      pym[a] = p[c - g.nx];
+      pzm[a] = p[c - g.nxy];
     }
   }
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
-    const int i = i0 + a;
-    u[c + a] = wall_u(g, i, j, k) ? T(0) : uu[a];
-    v[c + a] = wall_v(g, i, j, k) ? T(0) : vv[a];
-    w[c + a] = wall_w(g, i, j, k) ? T(0) : ww[a];
+    const int i = i0 + 32 * a;
+    if (rin && i >= 1 && i <= g.nx - 2) {
+      if (i > 1) uu[a] = T(double(uu[a]) - (pc[a] - pxm[a]) * inv_h);
+      if (j > 1) vv[a] = T(double(vv[a]) - (pc[a] - pym[a]) * inv_h);
+      if (k > 1) ww[a] = T(double(ww[a]) - (pc[a] - pzm[a]) * inv_h);
+    }
+    const int c = c0 + 32 * a;
+    u[c] = wall_u(g, i, j, k) ? T(0) : uu[a];
+    v[c] = wall_v(g, i, j, k) ? T(0) : vv[a];
+    w[c] = wall_w(g, i, j, k) ? T(0) : ww[a];
   }
 }
 
@@ -587,7 +589,7 @@ template <typename T>
 void launch_divergence(const Dims &g, const T *u, const T *v, const T *w, double *b,
                        double *partials, double *out2, cudaStream_t st) {
   const double inv_h = 1.0 / g.h;
-  if (g.nx % 4 == 0)
+  if (g.nx % 128 == 0)
     k_divergence_x4<T><<<kReduceBlocks, kBlock, 0, st>>>(g, u, v, w, b, partials, inv_h, g.h);
   else
     k_divergence<T><<<kReduceBlocks, kBlock, 0, st>>>(g, u, v, w, b, partials, inv_h, g.h);
@@ -597,8 +599,9 @@ void launch_divergence(const Dims &g, const T *u, const T *v, const T *w, double
 
 template <typename T>
 void launch_project(const Dims &g, T *u, T *v, T *w, const double *p, cudaStream_t st) {
-  if (g.nx % 4 == 0)
-    k_project_x4<T><<<(g.n / 4 + kBlock - 1) / kBlock, kBlock, 0, st>>>(g, u, v, w, p, 1.0 / g.h);
+  if (g.nx % 128 == 0)
+    k_project_x4<T><<<(g.n / 128 + kWarps - 1) / kWarps, kBlock, 0, st>>>(g, u, v, w, p,
+                                                                          1.0 / g.h);
   else
     k_project<T><<<column_grid(g), dim3(kTx, kTy), 0, st>>>(g, u, v, w, p, 1.0 / g.h);
 }

@@ -68,27 +68,91 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Copies rows [j0 - yh, j0 + kFy + yh) x columns [i0 - XH, i0 + kFx + XH) of
-// plane p of `src` into dst (row stride RW); cells outside the grid read 0.
-// With VEC the grid's nx is a multiple of V, so a 16-byte copy starting at a
-// column that is a multiple of V lies wholly inside or wholly outside a row.
+// One thread's part of staging a (kFy + 2*yh) x RW block of a plane: up to
+// two copies (RW / V chunks per row), their shared-memory offsets and their
+// offsets inside a plane, worked out once per CTA; per plane only the plane
+// offset and the plane's bounds change.
 template <typename T, bool VEC>
-__device__ __forceinline__ void stage_rows(T *dst, const T *__restrict__ src, const Dims &g,
-                                           int i0, int j0, int yh, int p) {
-  constexpr int V = VEC ? Staged<T>::V : 1;
-  constexpr int RW = Staged<T>::RW, XH = Staged<T>::XH, CPR = RW / V;
-  const int total = (kFy + 2 * yh) * CPR;
-  const bool pin = p >= 0 && p < g.nz;
-  for (int t = threadIdx.x; t < total; t += kFThreads) {
-    const int r = t / CPR;
-    const int m = t - r * CPR;
-    const int j = j0 - yh + r, i = i0 - XH + m * V;
-    const bool ok = pin && j >= 0 && j < g.ny && i >= 0 && i < g.nx;
-    const T *gp = ok ? src + (p * g.nxy + j * g.nx + i) : src;
-    T *sp = dst + r * RW + m * V;
-    if constexpr (VEC) cp_async16(sp, gp, ok);
-    else cp_async_small<int(sizeof(T))>(sp, gp, ok);
+struct StageDesc {
+  static constexpr int V = VEC ? Staged<T>::V : 1;
+  int soff[2], goff[2];
+  bool ok[2];
+  int n;
+  __device__ __forceinline__ StageDesc(const Dims &g, int i0, int j0, int yh) {
+    constexpr int RW = Staged<T>::RW, XH = Staged<T>::XH, CPR = RW / V;
+    const int total = (kFy + 2 * yh) * CPR;
+    n = 0;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int t = threadIdx.x + q * kFThreads;
+      soff[q] = 0;
+      goff[q] = 0;
+      ok[q] = false;
+      if (t < total) {
+        const int r = t / CPR;
+        const int m = t - r * CPR;
+        const int j = j0 - yh + r, i = i0 - XH + m * V;
+        soff[q] = r * RW + m * V;
+        ok[q] = j >= 0 && j < g.ny && i >= 0 && i < g.nx;
+        goff[q] = ok[q] ? j * g.nx + i : 0;
+        n = q + 1;
+      }
+    }
   }
+  // Copies plane p of src into dst (cells outside the grid read 0).
+  __device__ __forceinline__ void copy(T *dst, const T *__restrict__ src, const Dims &g,
+                                       int p) const {
+    const bool pin = p >= 0 && p < g.nz;
+    const T *plane = src + (pin ? p * g.nxy : 0);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      if (q >= n) break;
+      const bool okq = pin && ok[q];
+      if constexpr (VEC) cp_async16(dst + soff[q], okq ? plane + goff[q] : src, okq);
+      else cp_async_small<int(sizeof(T))>(dst + soff[q], okq ? plane + goff[q] : src, okq);
+    }
+  }
+};
+
+// Clamp bounds of sample_trilinear (src/fluid.rs:95-97) per axis, n - 1.500001,
+// computed once per CTA with the expression footprint3 uses.
+template <typename T>
+struct FpBounds {
+  T hx, hy, hz;
+  __device__ __forceinline__ explicit FpBounds(const Dims &g)
+      : hx(T(g.nx) - T(1.500001)), hy(T(g.ny) - T(1.500001)), hz(T(g.nz) - T(1.500001)) {}
+};
+
+// footprint3_at with the bounds precomputed: the same operations, so the same
+// corner and weights bit for bit.
+__device__ __forceinline__ void fp_axis(int i, double hi, double d, int &i0, double &t) {
+  const double xc = rs_clamp(double(i) - d, 0.5, hi);
+  i0 = static_cast<int>(floor(xc));
+  t = xc - double(i0);
+}
+__device__ __forceinline__ void fp_axis(int i, float hi, float d, int &i0, float &t) {
+  const float p = float(i) - d;
+  if (p < 0.5f) {
+    i0 = 0;
+    t = 0.5f;
+  } else if (p > hi) {
+    const float f = floorf(hi);
+    i0 = static_cast<int>(f);
+    t = hi - f;
+  } else {
+    const float f = floorf(-d);
+    i0 = i + static_cast<int>(f);
+    t = -d - f;
+  }
+}
+template <typename T>
+__device__ __forceinline__ Footprint3<T> fp_at(const FpBounds<T> &b, int i, int j, int k, T dx,
+                                               T dy, T dz) {
+  Footprint3<T> f;
+  fp_axis(i, b.hx, dx, f.i, f.tx);
+  fp_axis(j, b.hy, dy, f.j, f.ty);
+  fp_axis(k, b.hz, dz, f.k, f.tz);
+  return f;
 }
 
 // Cell t of the one-cell ring around the tile at (i0, j0).
@@ -140,6 +204,8 @@ struct McLayout {
 // is a velocity component, read from the staged velocity.  TEL (NF = 2,
 // field 0 = density): the telemetry sums over this CTA's cells go to
 // a.tel[7 * cta] as k_telemetry's partials.
+// Ring slots are tracked as plane offsets that advance by one slot per
+// iteration (no division); the plane pointers of an iteration are set once.
 template <typename T, int NF, bool SRC_IS_VEL, bool TEL, int S, bool VEC>
 __global__ void __launch_bounds__(kFThreads, NF == 1 ? 3 : 2)
     k_maccormack_fused(const __grid_constant__ McArgs<T> a) {
@@ -147,10 +213,10 @@ __global__ void __launch_bounds__(kFThreads, NF == 1 ? 3 : 2)
   using L = McLayout<T, NF, SRC_IS_VEL>;
   constexpr int RW = L::RW, XH = Staged<T>::XH, VYH = L::VYH, VROWS = L::VROWS;
   constexpr int SROWS = L::SROWS, VPL = L::VPL, SPL = L::SPL, FPL = L::FPL;
+  constexpr int PL = VPL + SPL;  // one ring slot: the velocity, then the fields
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *vring = reinterpret_cast<T *>(smem_raw);
-  T *sring = vring + S * VPL;
-  T *fring = sring + S * SPL;
+  T *ring = reinterpret_cast<T *>(smem_raw);
+  T *fring = ring + S * PL;
   const Dims &g = a.g;
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * kFx, j0 = blockIdx.y * kFy;
@@ -158,56 +224,59 @@ __global__ void __launch_bounds__(kFThreads, NF == 1 ? 3 : 2)
   const int k1 = min(k0 + a.kz, g.nz);
   const int mi = i0 + (tid & (kFx - 1)), mj = j0 + tid / kFx;
   const bool mine = mi < g.nx && mj < g.ny;
+  const FpBounds<T> fb_bounds(g);
+  const T wxl = T(1.5), wxh = T(g.nx) - T(2.5), wyh = T(g.ny) - T(2.5), wzh = T(g.nz) - T(2.5);
+  // field f of a slot starts SROWS*RW apart (velocity component vel_src when
+  // the field is a velocity component); rows start at y = j0 - 2
+  const int foff = SRC_IS_VEL ? a.vel_src * VROWS * RW : VPL;
+  constexpr int FSTRIDE = SROWS * RW;
 
-  auto slot = [](int p) { return (p + 2 * S) % S; };  // planes p >= -2
-  // staged velocity component c of plane p; row 0 is y = j0 - VYH, column 0 x = i0 - XH
-  auto vel = [&](int c, int p) -> const T * { return vring + slot(p) * VPL + c * VROWS * RW; };
-  // staged field f of plane p; row 0 is y = j0 - 2
-  auto field = [&](int f, int p) -> const T * {
-    if constexpr (SRC_IS_VEL) return vel(a.vel_src, p);
-    else return sring + slot(p) * SPL + f * SROWS * RW;
-  };
-  auto fwdp = [&](int f, int p) -> T * { return fring + ((p + 3) % 3) * FPL + f * kFh * kFw; };
-
-  auto stage = [&](int p) {
-    stage_rows<T, VEC>(vring + slot(p) * VPL, a.u, g, i0, j0, VYH, p);
-    stage_rows<T, VEC>(vring + slot(p) * VPL + VROWS * RW, a.v, g, i0, j0, VYH, p);
-    stage_rows<T, VEC>(vring + slot(p) * VPL + 2 * VROWS * RW, a.w, g, i0, j0, VYH, p);
+  const StageDesc<T, VEC> dvel(g, i0, j0, VYH);
+  const StageDesc<T, VEC> dsrc(g, i0, j0, 2);
+  auto stage = [&](T *slotp, int p) {
+    dvel.copy(slotp, a.u, g, p);
+    dvel.copy(slotp + VROWS * RW, a.v, g, p);
+    dvel.copy(slotp + 2 * VROWS * RW, a.w, g, p);
     if constexpr (!SRC_IS_VEL) {
 #pragma unroll
-      for (int f = 0; f < NF; ++f)
-        stage_rows<T, VEC>(sring + slot(p) * SPL + f * SROWS * RW, a.src[f], g, i0, j0, 2, p);
+      for (int f = 0; f < NF; ++f) dsrc.copy(slotp + VPL + f * FSTRIDE, a.src[f], g, p);
     }
     cp_async_commit();
   };
+  auto next_slot = [&](T *sp) { return sp + PL == ring + S * PL ? ring : sp + PL; };
 
-  // fwd = SL(src, dt) at cell (ci, cj, p) (advect_semi_lagrangian,
-  // src/fluid.rs:153-167); for the thread's own cell (own), also the min/max
-  // of the same 8 corners (stencil_minmax, :131-150), the bounds of its clamp.
-  auto fwd_cell = [&](int ci, int cj, int p, bool own, T (&lo)[NF], T (&hi)[NF]) {
+  // fwd = SL(src, dt) at cell (ci, cj) of plane p (advect_semi_lagrangian,
+  // src/fluid.rs:153-167) into fo of the fwd plane F.  vp: the staged plane
+  // p; vm, vq: planes p-1 and p+1 (for the field corners).  For the thread's
+  // own cell (own), also the min/max of the same 8 corners (stencil_minmax,
+  // :131-150), the bounds of its clamp.
+  auto fwd_cell = [&](int ci, int cj, int p, const T *vm, const T *vp, const T *vq, T *F,
+                      bool own, T (&lo)[NF], T (&hi)[NF]) {
     T res[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) res[f] = T(0);
     if (interior(g, ci, cj, p)) {
       const int vo = (cj - j0 + VYH) * RW + (ci - i0 + XH);
-      const T uc = vel(0, p)[vo], vc = vel(1, p)[vo], wc = vel(2, p)[vo];
+      const T uc = vp[vo], vc = vp[VROWS * RW + vo], wc = vp[2 * VROWS * RW + vo];
       const Footprint3<T> fp =
-          footprint3_at(g, ci, cj, p, a.scale_f * uc, a.scale_f * vc, a.scale_f * wc);
+          fp_at(fb_bounds, ci, cj, p, a.scale_f * uc, a.scale_f * vc, a.scale_f * wc);
       const bool staged = fp.i >= i0 - XH && fp.i + 1 < i0 + kFx + XH && fp.j >= j0 - 2 &&
-                          fp.j + 1 < j0 + kFy + 2 && fp.k >= p - 1 && fp.k + 1 <= p + 1;
+                          fp.j + 1 < j0 + kFy + 2 && fp.k >= p - 1 && fp.k <= p;
+      const int o = (fp.j - j0 + 2) * RW + (fp.i - i0 + XH) + foff;
+      const T *z0 = (fp.k == p - 1 ? vm : vp) + o;
+      const T *z1 = (fp.k == p - 1 ? vp : vq) + o;
 #pragma unroll
       for (int f = 0; f < NF; ++f) {
         T c[8];
         if (staged) {
-          const int o = (fp.j - j0 + 2) * RW + (fp.i - i0 + XH);
-          const T *s0 = field(f, fp.k) + o, *s1 = field(f, fp.k + 1) + o;
+          const T *s0 = z0 + f * FSTRIDE, *s1 = z1 + f * FSTRIDE;
           c[0] = s0[0]; c[1] = s0[1]; c[2] = s0[RW]; c[3] = s0[RW + 1];
           c[4] = s1[0]; c[5] = s1[1]; c[6] = s1[RW]; c[7] = s1[RW + 1];
         } else {
-          const T *s = a.src[f] + fp.base(g);
-          c[0] = __ldg(s); c[1] = __ldg(s + 1); c[2] = __ldg(s + g.nx);
-          c[3] = __ldg(s + g.nx + 1); c[4] = __ldg(s + g.nxy); c[5] = __ldg(s + g.nxy + 1);
-          c[6] = __ldg(s + g.nxy + g.nx); c[7] = __ldg(s + g.nxy + g.nx + 1);
+          const T *sg = a.src[f] + fp.base(g);
+          c[0] = __ldg(sg); c[1] = __ldg(sg + 1); c[2] = __ldg(sg + g.nx);
+          c[3] = __ldg(sg + g.nx + 1); c[4] = __ldg(sg + g.nxy); c[5] = __ldg(sg + g.nxy + 1);
+          c[6] = __ldg(sg + g.nxy + g.nx); c[7] = __ldg(sg + g.nxy + g.nx + 1);
         }
         res[f] = lerp8(c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], fp.tx, fp.ty, fp.tz);
         if (own) {
@@ -224,19 +293,21 @@ __global__ void __launch_bounds__(kFThreads, NF == 1 ? 3 : 2)
     }
     const int fo = (cj - j0 + 1) * kFw + (ci - i0 + 1);
 #pragma unroll
-    for (int f = 0; f < NF; ++f) fwdp(f, p)[fo] = res[f];
+    for (int f = 0; f < NF; ++f) F[f * kFh * kFw + fo] = res[f];
   };
 
+  // This thread's ring cell (threads below kFHalo), found once.
+  int hi_i = 0, hi_j = 0;
+  if (tid < kFHalo) halo_cell(tid, i0, j0, hi_i, hi_j);
   // fwd of plane p on the tile and its one-cell ring (planes outside the grid
   // are never sampled: every footprint lies inside it).
-  auto fwd_plane = [&](int p, T (&lo)[NF], T (&hi)[NF]) {
+  auto fwd_plane = [&](int p, const T *vm, const T *vp, const T *vq, T *F, T (&lo)[NF],
+                       T (&hi)[NF]) {
     if (p < 0 || p >= g.nz) return;
-    if (mine) fwd_cell(mi, mj, p, true, lo, hi);
+    if (mine) fwd_cell(mi, mj, p, vm, vp, vq, F, true, lo, hi);
     if (tid < kFHalo) {
-      int hi_, hj;
-      halo_cell(tid, i0, j0, hi_, hj);
       T dl[NF], dh[NF];
-      fwd_cell(hi_, hj, p, false, dl, dh);
+      fwd_cell(hi_i, hi_j, p, vm, vp, vq, F, false, dl, dh);
     }
   };
 
@@ -255,18 +326,35 @@ __global__ void __launch_bounds__(kFThreads, NF == 1 ? 3 : 2)
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   double peak = 0.0;
 
-  for (int p = k0 - 2; p <= k0 + S - 3; ++p) stage(p);
+  // slot of plane k0-2 is ring[0]; plane k0-2+t sits in slot t mod S
+  {
+    T *sp = ring;
+    for (int p = k0 - 2; p <= k0 + S - 3; ++p) {
+      stage(sp, p);
+      sp += PL;
+    }
+  }
+  T *sm2 = ring;                 // plane k-2 (k = k0)
+  T *sm1 = ring + PL;            // k-1
+  T *s0 = ring + 2 * PL;         // k
+  T *s1 = ring + 3 * PL;         // k+1
+  T *s2 = ring + 4 * PL;         // k+2
+  T *F0 = fring, *F1 = fring + FPL, *F2 = fring + 2 * FPL;  // fwd of planes k-1, k, k+1
   cp_async_wait<S - 4>();  // planes k0-2 .. k0+1 have landed
   __syncthreads();
-  fwd_plane(k0 - 1, lo_nxt, hi_nxt);  // ring plane only; the bounds are not used
-  fwd_plane(k0, lo_cur, hi_cur);
+  fwd_plane(k0 - 1, sm2, sm1, s0, F0, lo_nxt, hi_nxt);  // ring plane only
+  fwd_plane(k0, sm1, s0, s1, F1, lo_cur, hi_cur);
 
   for (int k = k0; k < k1; ++k) {
     cp_async_wait<S - 5>();  // plane k+2 has landed
     __syncthreads();         // ... for every thread; iteration k-1 is done with its planes
-    fwd_plane(k + 1, lo_nxt, hi_nxt);
+    fwd_plane(k + 1, s0, s1, s2, F2, lo_nxt, hi_nxt);
     __syncthreads();         // fwd of plane k+1 is visible
-    stage(k + S - 2);        // into the slot of plane k-2, last read in iteration k-1
+    {
+      // plane k+S-2 goes into the slot of plane k-2, last read in iteration k-1
+      T *sp = sm2;
+      stage(sp, k + S - 2);
+    }
     if (mine) {
       T res[NF];
 #pragma unroll
@@ -274,28 +362,30 @@ __global__ void __launch_bounds__(kFThreads, NF == 1 ? 3 : 2)
       const int vo = (mj - j0 + VYH) * RW + (mi - i0 + XH);
       const bool inner = interior(g, mi, mj, k);
       if (inner) {
-        const T uc = vel(0, k)[vo], vc = vel(1, k)[vo], wc = vel(2, k)[vo];
+        const T uc = s0[vo], vc = s0[VROWS * RW + vo], wc = s0[2 * VROWS * RW + vo];
         const T bx = T(mi) - a.scale_f * uc;
         const T by = T(mj) - a.scale_f * vc;
         const T bz = T(k) - a.scale_f * wc;
-        const bool near_wall = bx < T(1.5) || bx > T(g.nx) - T(2.5) || by < T(1.5) ||
-                               by > T(g.ny) - T(2.5) || bz < T(1.5) || bz > T(g.nz) - T(2.5);
+        const bool near_wall = bx < wxl || bx > wxh || by < wxl || by > wyh || bz < wxl ||
+                               bz > wzh;
         const int fo = (mj - j0 + 1) * kFw + (mi - i0 + 1);
         if (near_wall) {
 #pragma unroll
-          for (int f = 0; f < NF; ++f) res[f] = fwdp(f, k)[fo] * a.diss[f];
+          for (int f = 0; f < NF; ++f) res[f] = F1[f * kFh * kFw + fo] * a.diss[f];
         } else {
           const Footprint3<T> fb =
-              footprint3_at(g, mi, mj, k, a.scale_b * uc, a.scale_b * vc, a.scale_b * wc);
+              fp_at(fb_bounds, mi, mj, k, a.scale_b * uc, a.scale_b * vc, a.scale_b * wc);
           const bool staged = fb.i >= i0 - 1 && fb.i + 1 <= i0 + kFx && fb.j >= j0 - 1 &&
-                              fb.j + 1 <= j0 + kFy && fb.k >= k - 1 && fb.k + 1 <= k + 1;
-          const int so = (mj - j0 + 2) * RW + (mi - i0 + XH);
+                              fb.j + 1 <= j0 + kFy && fb.k >= k - 1 && fb.k <= k;
+          const int o = (fb.j - j0 + 1) * kFw + (fb.i - i0 + 1);
+          const T *z0 = (fb.k == k - 1 ? F0 : F1) + o;
+          const T *z1 = (fb.k == k - 1 ? F1 : F2) + o;
+          const int so = (mj - j0 + 2) * RW + (mi - i0 + XH) + foff;
 #pragma unroll
           for (int f = 0; f < NF; ++f) {
             T bwd;
             if (staged) {
-              const int o = (fb.j - j0 + 1) * kFw + (fb.i - i0 + 1);
-              const T *f0 = fwdp(f, fb.k) + o, *f1 = fwdp(f, fb.k + 1) + o;
+              const T *f0 = z0 + f * kFh * kFw, *f1 = z1 + f * kFh * kFw;
               bwd = lerp8(f0[0], f0[1], f0[kFw], f0[kFw + 1], f1[0], f1[1], f1[kFw],
                           f1[kFw + 1], fb.tx, fb.ty, fb.tz);
             } else {
@@ -307,8 +397,8 @@ __global__ void __launch_bounds__(kFThreads, NF == 1 ? 3 : 2)
                           fwd_global(f, fb.i, fb.j + 1, fb.k + 1),
                           fwd_global(f, fb.i + 1, fb.j + 1, fb.k + 1), fb.tx, fb.ty, fb.tz);
             }
-            const T fc = fwdp(f, k)[fo];
-            const T mc = fc + T(0.5) * (field(f, k)[so] - bwd);
+            const T fc = F1[f * kFh * kFw + fo];
+            const T mc = fc + T(0.5) * (s0[so + f * FSTRIDE] - bwd);
             res[f] = rs_clamp(mc, lo_cur[f], hi_cur[f]) * a.diss[f];
           }
         }
@@ -321,17 +411,17 @@ __global__ void __launch_bounds__(kFThreads, NF == 1 ? 3 : 2)
       }
       if constexpr (TEL) {
         if (inner) {  // compute_telemetry (src/fluid.rs:613-672) at this cell
-          const double uc = vel(0, k)[vo], vc = vel(1, k)[vo], wc = vel(2, k)[vo];
+          const T *U = s0, *Vv = s0 + VROWS * RW, *W = s0 + 2 * VROWS * RW;
+          const double uc = U[vo], vc = Vv[vo], wc = W[vo];
           const double u2 = uc * uc + vc * vc + wc * wc;
           acc[0] += 0.5 * u2 * a.dv;
-          const double dw_dy =
-              (double(vel(2, k)[vo + RW]) - double(vel(2, k)[vo - RW])) * a.inv_2h;
-          const double dv_dz = (double(vel(1, k + 1)[vo]) - double(vel(1, k - 1)[vo])) * a.inv_2h;
-          const double du_dz = (double(vel(0, k + 1)[vo]) - double(vel(0, k - 1)[vo])) * a.inv_2h;
-          const double dw_dx = (double(vel(2, k)[vo + 1]) - double(vel(2, k)[vo - 1])) * a.inv_2h;
-          const double dv_dx = (double(vel(1, k)[vo + 1]) - double(vel(1, k)[vo - 1])) * a.inv_2h;
-          const double du_dy =
-              (double(vel(0, k)[vo + RW]) - double(vel(0, k)[vo - RW])) * a.inv_2h;
+          const double dw_dy = (double(W[vo + RW]) - double(W[vo - RW])) * a.inv_2h;
+          const double dv_dz =
+              (double(s1[VROWS * RW + vo]) - double(sm1[VROWS * RW + vo])) * a.inv_2h;
+          const double du_dz = (double(s1[vo]) - double(sm1[vo])) * a.inv_2h;
+          const double dw_dx = (double(W[vo + 1]) - double(W[vo - 1])) * a.inv_2h;
+          const double dv_dx = (double(Vv[vo + 1]) - double(Vv[vo - 1])) * a.inv_2h;
+          const double du_dy = (double(U[vo + RW]) - double(U[vo - RW])) * a.inv_2h;
           const double ox = dw_dy - dv_dz;
           const double oy = du_dz - dw_dx;
           const double oz = dv_dx - du_dy;
@@ -357,6 +447,18 @@ __global__ void __launch_bounds__(kFThreads, NF == 1 ? 3 : 2)
       lo_cur[f] = lo_nxt[f];
       hi_cur[f] = hi_nxt[f];
     }
+    // advance the ring by one plane
+    T *old = sm2;
+    sm2 = sm1;
+    sm1 = s0;
+    s0 = s1;
+    s1 = s2;
+    s2 = next_slot(s2);
+    (void)old;
+    T *ft = F0;
+    F0 = F1;
+    F1 = F2;
+    F2 = ft;
   }
   cp_async_wait<0>();  // no copy outlives the CTA
   if constexpr (TEL) {
@@ -397,9 +499,10 @@ __global__ void __launch_bounds__(kFThreads, 3)
   static_assert(S >= 5, "the ring holds planes k-2 .. k+2 plus at least one ahead");
   using L = ForcesLayout<T>;
   constexpr int RW = L::RW, XH = Staged<T>::XH, VROWS = L::VROWS, VPL = L::VPL, MPL = L::MPL;
+  constexpr int CS = VROWS * RW;  // one velocity component of a slot
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *vring = reinterpret_cast<T *>(smem_raw);
-  T *mring = vring + S * VPL;
+  T *ring = reinterpret_cast<T *>(smem_raw);
+  T *mring = ring + S * VPL;
   const Dims &g = a.g;
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * kFx, j0 = blockIdx.y * kFy;
@@ -408,28 +511,28 @@ __global__ void __launch_bounds__(kFThreads, 3)
   const int mi = i0 + (tid & (kFx - 1)), mj = j0 + tid / kFx;
   const bool mine = mi < g.nx && mj < g.ny;
 
-  auto slot = [](int p) { return (p + 2 * S) % S; };
-  auto vel = [&](int c, int p) -> const T * { return vring + slot(p) * VPL + c * VROWS * RW; };
-  auto mag = [&](int p) -> T * { return mring + ((p + 3) % 3) * MPL; };
-  auto stage = [&](int p) {
-    stage_rows<T, VEC>(vring + slot(p) * VPL, a.u, g, i0, j0, 2, p);
-    stage_rows<T, VEC>(vring + slot(p) * VPL + VROWS * RW, a.v, g, i0, j0, 2, p);
-    stage_rows<T, VEC>(vring + slot(p) * VPL + 2 * VROWS * RW, a.w, g, i0, j0, 2, p);
+  const StageDesc<T, VEC> dvel(g, i0, j0, 2);
+  auto stage = [&](T *sp, int p) {
+    dvel.copy(sp, a.u, g, p);
+    dvel.copy(sp + CS, a.v, g, p);
+    dvel.copy(sp + 2 * CS, a.w, g, p);
     cp_async_commit();
   };
+  auto next_slot = [&](T *sp) { return sp + VPL == ring + S * VPL ? ring : sp + VPL; };
 
-  // Central-difference curl and |w| at (ci, cj, p) on the interior
-  // (src/fluid.rs:260-281); 0 elsewhere.
-  auto curl_cell = [&](int ci, int cj, int p, T &ox, T &oy, T &oz) -> T {
+  // Central-difference curl and |w| at (ci, cj) of plane p on the interior
+  // (src/fluid.rs:260-281), 0 elsewhere; vm, vp, vq: staged planes p-1, p, p+1.
+  auto curl_cell = [&](int ci, int cj, int p, const T *vm, const T *vp, const T *vq, T &ox,
+                       T &oy, T &oz) -> T {
     if (!interior(g, ci, cj, p)) {
       ox = oy = oz = T(0);
       return T(0);
     }
     const int o = (cj - j0 + 2) * RW + (ci - i0 + XH);
-    const T *U = vel(0, p) + o, *Vv = vel(1, p) + o, *W = vel(2, p) + o;
+    const T *U = vp + o, *Vv = vp + CS + o, *W = vp + 2 * CS + o;
     const T dw_dy = (W[RW] - W[-RW]) * a.inv_2h;
-    const T dv_dz = (vel(1, p + 1)[o] - vel(1, p - 1)[o]) * a.inv_2h;
-    const T du_dz = (vel(0, p + 1)[o] - vel(0, p - 1)[o]) * a.inv_2h;
+    const T dv_dz = (vq[CS + o] - vm[CS + o]) * a.inv_2h;
+    const T du_dz = (vq[o] - vm[o]) * a.inv_2h;
     const T dw_dx = (W[1] - W[-1]) * a.inv_2h;
     const T dv_dx = (Vv[1] - Vv[-1]) * a.inv_2h;
     const T du_dy = (U[RW] - U[-RW]) * a.inv_2h;
@@ -438,23 +541,33 @@ __global__ void __launch_bounds__(kFThreads, 3)
     oz = dv_dx - du_dy;
     return sqrt(ox * ox + oy * oy + oz * oz);
   };
-  auto curl_plane = [&](int p, T &ox, T &oy, T &oz) {
+  int hi_i = 0, hi_j = 0;
+  if (tid < kFHalo) halo_cell(tid, i0, j0, hi_i, hi_j);
+  auto curl_plane = [&](int p, const T *vm, const T *vp, const T *vq, T *M, T &ox, T &oy,
+                        T &oz) {
     if (p < 0 || p >= g.nz) return;  // never read: confinement touches planes 1..nz-2
-    if (mine) mag(p)[(mj - j0 + 1) * kFw + (mi - i0 + 1)] = curl_cell(mi, mj, p, ox, oy, oz);
+    if (mine) M[(mj - j0 + 1) * kFw + (mi - i0 + 1)] = curl_cell(mi, mj, p, vm, vp, vq, ox, oy, oz);
     if (tid < kFHalo) {
-      int hi_, hj;
-      halo_cell(tid, i0, j0, hi_, hj);
       T x_, y_, z_;
-      mag(p)[(hj - j0 + 1) * kFw + (hi_ - i0 + 1)] = curl_cell(hi_, hj, p, x_, y_, z_);
+      M[(hi_j - j0 + 1) * kFw + (hi_i - i0 + 1)] = curl_cell(hi_i, hi_j, p, vm, vp, vq, x_, y_, z_);
     }
   };
 
   T ox = T(0), oy = T(0), oz = T(0), nox = T(0), noy = T(0), noz = T(0);
-  for (int p = k0 - 2; p <= k0 + S - 3; ++p) stage(p);
+  {
+    T *sp = ring;
+    for (int p = k0 - 2; p <= k0 + S - 3; ++p) {
+      stage(sp, p);
+      sp += VPL;
+    }
+  }
+  T *sm2 = ring, *sm1 = ring + VPL, *s0 = ring + 2 * VPL, *s1 = ring + 3 * VPL,
+    *s2 = ring + 4 * VPL;
+  T *M0 = mring, *M1 = mring + MPL, *M2 = mring + 2 * MPL;  // |w| of planes k-1, k, k+1
   cp_async_wait<S - 4>();
   __syncthreads();
-  curl_plane(k0 - 1, nox, noy, noz);
-  curl_plane(k0, ox, oy, oz);
+  curl_plane(k0 - 1, sm2, sm1, s0, M0, nox, noy, noz);
+  curl_plane(k0, sm1, s0, s1, M1, ox, oy, oz);
 
   for (int k = k0; k < k1; ++k) {
     const int c = (k * g.ny + mj) * g.nx + mi;
@@ -465,18 +578,18 @@ __global__ void __launch_bounds__(kFThreads, 3)
     }
     cp_async_wait<S - 5>();
     __syncthreads();
-    curl_plane(k + 1, nox, noy, noz);
+    curl_plane(k + 1, s0, s1, s2, M2, nox, noy, noz);
     __syncthreads();
-    stage(k + S - 2);
+    stage(sm2, k + S - 2);
     if (mine) {  // cell_confine_buoy at (mi, mj, k)
       const int o = (mj - j0 + 2) * RW + (mi - i0 + XH);
-      T uu = vel(0, k)[o], vv = vel(1, k)[o], ww = vel(2, k)[o];
+      T uu = s0[o], vv = s0[CS + o], ww = s0[2 * CS + o];
       if (mi >= 2 && mi <= g.nx - 3 && mj >= 2 && mj <= g.ny - 3 && k >= 2 && k <= g.nz - 3) {
         const int mo = (mj - j0 + 1) * kFw + (mi - i0 + 1);
-        const T *M = mag(k) + mo;
+        const T *M = M1 + mo;
         const T gx = (M[1] - M[-1]) * a.inv_2h;
         const T gy = (M[kFw] - M[-kFw]) * a.inv_2h;
-        const T gz = (mag(k + 1)[mo] - mag(k - 1)[mo]) * a.inv_2h;
+        const T gz = (M2[mo] - M0[mo]) * a.inv_2h;
         const T glen = sqrt(gx * gx + gy * gy + gz * gz) + T(1e-10);
         const T nx_ = gx / glen, ny_ = gy / glen, nz_ = gz / glen;
         const T fx = a.eps_h * (ny_ * oz - nz_ * oy);
@@ -497,6 +610,15 @@ __global__ void __launch_bounds__(kFThreads, 3)
     ox = nox;
     oy = noy;
     oz = noz;
+    sm2 = sm1;
+    sm1 = s0;
+    s0 = s1;
+    s1 = s2;
+    s2 = next_slot(s2);
+    T *mt = M0;
+    M0 = M1;
+    M1 = M2;
+    M2 = mt;
   }
   cp_async_wait<0>();
 }
