@@ -117,7 +117,6 @@ struct afl_solver {
   // Poisson vectors: FP64 -> r, d0, d1, q (double); MIXED -> r, e, d0, d1, q (float)
   void *cg[5] = {};
   double *partials = nullptr;     // kReduceBlocks * kReduceMaxVals
-  double *tel_partials = nullptr; // 7 per CTA of the fused density/temperature advection
   double *scal = nullptr;         // [0..1] divergence {rms,||b||}, [2..9] telemetry, [10] max
   double *tel = nullptr;          // run telemetry, 8 doubles per step
   afl::SolveReport *reports = nullptr;  // run reports, one per step
@@ -271,43 +270,16 @@ afl_status launch_check() {
 }
 
 // ---- stages, generic over the field type ------------------------------------
-// advect_maccormack_in_place (src/fluid.rs:170-234) of one field: one fused
-// launch into the spare buffer, which then becomes the field.
 template <typename T>
 afl_status stage_advect(afl_solver *s, int kind, double dt, double diss) {
   const int f = (kind >= 0 && kind <= 3) ? kind : 4;  // `_ =>` arm: temperature
   const T *u = s->F<T>(0), *v = s->F<T>(1), *w = s->F<T>(2);
-  const T *src[2] = {s->F<T>(f), nullptr};
-  T *out[2] = {static_cast<T *>(s->tmp_out), nullptr};
-  const double diss2[2] = {diss, 0.0};
-  StageTimer timer(s, AFL_STAGE_ADVECT, 1);
-  afl::launch_advect_fused<T>(s->g, u, v, w, 1, src, out, diss2, f >= 3, f <= 2 ? f : -1, dt,
-                              nullptr, s->stream);
+  const T *src = s->F<T>(f);
+  T *fwd = static_cast<T *>(s->tmp_fwd), *out = static_cast<T *>(s->tmp_out);
+  StageTimer timer(s, AFL_STAGE_ADVECT, 2);
+  afl::launch_advect_fwd<T>(s->g, u, v, w, src, fwd, dt, s->stream);
+  afl::launch_advect_mc<T>(s->g, u, v, w, src, fwd, out, dt, diss, f >= 3, s->stream);
   std::swap(s->fld[f], s->tmp_out);
-  return launch_check();
-}
-
-// The end of step() (src/fluid.rs:607-610): density (dissipation 0.996) and
-// temperature (0.985) advected in one fused launch that also sums the
-// telemetry of the final state; the finalize kernel writes its 8 doubles.
-template <typename T>
-afl_status stage_advect_scalars_telemetry(afl_solver *s, double dt, double time_sec,
-                                          double *out8) {
-  const T *u = s->F<T>(0), *v = s->F<T>(1), *w = s->F<T>(2);
-  const T *src[2] = {s->F<T>(3), s->F<T>(4)};
-  T *out[2] = {static_cast<T *>(s->tmp_out), static_cast<T *>(s->tmp_fwd)};
-  const double diss[2] = {0.996, 0.985};
-  {
-    StageTimer timer(s, AFL_STAGE_ADVECT, 1);
-    afl::launch_advect_fused<T>(s->g, u, v, w, 2, src, out, diss, true, -1, dt,
-                                s->tel_partials, s->stream);
-  }
-  std::swap(s->fld[3], s->tmp_out);
-  std::swap(s->fld[4], s->tmp_fwd);
-  AFL_TRY(launch_check());
-  StageTimer timer(s, AFL_STAGE_TELEMETRY, 1);
-  afl::launch_telemetry_finalize(s->tel_partials, afl::fused_ctas(s->g), time_sec, out8,
-                                 s->stream);
   return launch_check();
 }
 
@@ -318,17 +290,34 @@ afl_status stage_wall_bc(afl_solver *s) {
   return launch_check();
 }
 
-// apply_buoyancy_and_vorticity_confinement (src/fluid.rs:256-330): one fused
-// launch writes the new velocity into three spare buffers, which then become
-// u, v, w (the curl never reaches memory).
+// apply_buoyancy_and_vorticity_confinement (src/fluid.rs:256-330).  Grids
+// whose stage arrays exceed twice the L2 cache: one fused, shared-memory
+// staged launch writes the new velocity into three spare buffers, which then
+// become u, v, w (the curl never reaches memory).  Smaller grids, whose
+// arrays L2 holds: the curl kernel and the confinement kernel, one thread per
+// cell (at these sizes the extra curl traffic stays in L2 and the simple
+// kernels' occupancy wins).
 template <typename T>
 afl_status stage_buoyancy_vorticity(afl_solver *s, double dt) {
-  StageTimer timer(s, AFL_STAGE_FORCES, 1);
-  afl::launch_forces_fused<T>(s->g, s->F<T>(0), s->F<T>(1), s->F<T>(2), s->F<T>(3), s->F<T>(4),
-                              static_cast<T *>(s->curl[0]), static_cast<T *>(s->curl[1]),
-                              static_cast<T *>(s->curl[2]), dt, s->params.vorticity_eps,
-                              s->params.buoyancy_beta, s->params.gravity_alpha, s->stream);
-  for (int f = 0; f < 3; ++f) std::swap(s->fld[f], s->curl[f]);
+  if (afl::streams_through_hbm(s->g, 8 * sizeof(T))) {
+    StageTimer timer(s, AFL_STAGE_FORCES, 1);
+    afl::launch_forces_fused<T>(s->g, s->F<T>(0), s->F<T>(1), s->F<T>(2), s->F<T>(3),
+                                s->F<T>(4), static_cast<T *>(s->curl[0]),
+                                static_cast<T *>(s->curl[1]), static_cast<T *>(s->curl[2]), dt,
+                                s->params.vorticity_eps, s->params.buoyancy_beta,
+                                s->params.gravity_alpha, s->stream);
+    for (int f = 0; f < 3; ++f) std::swap(s->fld[f], s->curl[f]);
+    return launch_check();
+  }
+  T *c[4] = {static_cast<T *>(s->curl[0]), static_cast<T *>(s->curl[1]),
+             static_cast<T *>(s->curl[2]), static_cast<T *>(s->curl[3])};
+  StageTimer timer(s, AFL_STAGE_FORCES, 2);
+  afl::launch_curl<T>(s->g, s->F<T>(0), s->F<T>(1), s->F<T>(2), c[0], c[1], c[2], c[3],
+                      s->stream);
+  afl::launch_confine_buoy<T>(s->g, s->F<T>(0), s->F<T>(1), s->F<T>(2), s->F<T>(3),
+                              s->F<T>(4), c[0], c[1], c[2], c[3], dt,
+                              s->params.vorticity_eps, s->params.buoyancy_beta,
+                              s->params.gravity_alpha, s->stream);
   return launch_check();
 }
 
@@ -485,7 +474,9 @@ afl_status stage_step(afl_solver *s, double dt, double time_sec, double *tel8,
   // The confinement kernel ends with the wall BC, so project's leading
   // enforce_wall_velocity_bc (src/fluid.rs:497) is a no-op here and skipped.
   AFL_TRY(stage_project<T>(s, false, rep));
-  return stage_advect_scalars_telemetry<T>(s, dt, time_sec, tel8);
+  AFL_TRY(stage_advect<T>(s, 3, dt, 0.996));
+  AFL_TRY(stage_advect<T>(s, 4, dt, 0.985));
+  return stage_telemetry<T>(s, time_sec, tel8);
 }
 
 template <typename Fn>
@@ -681,8 +672,6 @@ afl_status afl_create(size_t nx, size_t ny, size_t nz, const afl_params *params,
   if (st == AFL_OK)
     st = alloc_as(s, &s->partials, sizeof(double) * afl::kReduceBlocks * afl::kReduceMaxVals);
   if (st == AFL_OK) st = alloc_as(s, &s->scal, sizeof(double) * 16);
-  if (st == AFL_OK)
-    st = alloc_as(s, &s->tel_partials, sizeof(double) * 7 * afl::fused_ctas(s->g));
   if (st == AFL_OK) st = alloc_as(s, &s->sticky, sizeof(int) * 4);
   // persistent-kernel state: the CTA bound is the largest co-resident grid
   int maxb = std::max(std::max(afl::persistent_blocks_cg_f64(), afl::persistent_blocks_sor_f64()),

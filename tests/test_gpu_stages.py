@@ -76,19 +76,17 @@ def test_advect_maccormack(af, oracle, shape, kind, precision):
     same(g, o, [name, "u", "v", "w"], precision, tol=2e-6)
 
 
-# Grids of several 32 x 8 tiles and z chunks for the fused, shared-memory
-# staged kernels: rows 16-byte aligned or not (nx a multiple of 4, even, odd),
-# and ragged tiles in x and y.
-FUSED_SHAPES = [(64, 24, 40), (70, 36, 33), (45, 17, 50)]
+# Grids of several 32 x 8 tiles and z chunks: rows 16-byte aligned or not (nx
+# a multiple of 4, even, odd), ragged tiles in x and y.
+TILE_SHAPES = [(64, 24, 40), (70, 36, 33), (45, 17, 50)]
 
 
-@pytest.mark.parametrize("shape", FUSED_SHAPES)
+@pytest.mark.parametrize("shape", TILE_SHAPES)
 @pytest.mark.parametrize("steps_per_cell", [0.4, 3.0])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_fused_advection_tiles(af, oracle, shape, steps_per_cell, precision):
-    """The fused MacCormack kernel over many tiles and z chunks: at 0.4 cells
-    per step every footprint lies in the staged tile, at 3 cells most leave it
-    and take the global-memory path.  FP64 matches the oracle bit for bit."""
+def test_advection_tiles(af, oracle, shape, steps_per_cell, precision):
+    """Advection of all five fields over many tiles, at 0.4 and 3 cells per
+    step; FP64 matches the oracle bit for bit."""
     g, o = pair(af, oracle, shape, seed=41, vel_scale=1.0, precision=precision)
     dt = steps_per_cell * g.h
     for kind in range(5):
@@ -97,14 +95,35 @@ def test_fused_advection_tiles(af, oracle, shape, steps_per_cell, precision):
     same(g, o, ["u", "v", "w", "density", "temperature"], precision, tol=2e-6)
 
 
-@pytest.mark.parametrize("shape", FUSED_SHAPES)
-@pytest.mark.parametrize("precision", [0, 1])
-def test_fused_forces_tiles(af, oracle, shape, precision):
+# Grids whose stage arrays exceed twice the L2 cache, where the solver runs
+# the shared-memory-staged forces kernel (16-byte rows, and odd nx for the
+# element-wise copies) and the x4 divergence/projection kernels.
+STREAM_FORCES = [((176, 160, 160), 0), ((177, 160, 160), 0), ((224, 200, 200), 1)]
+
+
+@pytest.mark.parametrize("shape,precision", STREAM_FORCES,
+                         ids=["176x160x160-fp64", "177x160x160-fp64", "224x200x200-mixed"])
+def test_staged_forces_large(af, oracle, shape, precision):
     g, o = pair(af, oracle, shape, seed=43, vel_scale=0.5, precision=precision,
                 vorticity_eps=0.3, buoyancy_beta=0.4, gravity_alpha=0.08)
     g.apply_buoyancy_and_vorticity_confinement(0.02)
     o.apply_buoyancy_and_vorticity_confinement(0.02)
     same(g, o, VEL, precision, tol=1e-5)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_x4_divergence_and_projection_large(af, oracle, precision):
+    """256 x 256 x 208: the divergence and the projection gradient on runs of
+    4 cells per thread (FP64 bit for bit; mixed within 1e-5)."""
+    shape = (256, 256, 208)
+    g, o = pair(af, oracle, shape, seed=47, vel_scale=0.5, precision=precision,
+                solver_kind=1, solver_iters=2, sor_omega=1.7)
+    rg, ro = g.compute_divergence_norm(), o.compute_divergence_norm()
+    assert abs(rg - ro) <= (1e-13 if precision == 0 else 1e-5) * ro
+    same(g, o, ["divergence"], precision, tol=1e-5)
+    g.project()
+    o.project()
+    same(g, o, ["u", "v", "w", "pressure"], precision, tol=1e-5)
 
 
 @pytest.mark.parametrize("shape", SHAPES)
