@@ -73,14 +73,12 @@ void launch_convert_f32_to_f64(const float *src, double *dst, int n, cudaStream_
   k_f32_to_f64<<<kReduceBlocks, kBlock, 0, st>>>(src, dst, n);
 }
 
-bool streams_through_hbm(const Dims &g, size_t bytes_per_cell) {
-  int dev = 0, l2 = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess || l2 <= 0)
-    l2 = 126 << 20;
-  return static_cast<double>(g.n) * static_cast<double>(bytes_per_cell) >
-         2.0 * static_cast<double>(l2);
+void launch_telemetry_finalize(const double *partials, int nparts, double time_sec,
+                               double *out8, cudaStream_t st) {
+  k_telemetry_finalize<<<1, kBlock, 0, st>>>(partials, nparts, time_sec, out8);
 }
+
+int fused_ctas(const Dims &g) { return fused_ctas_of(g); }
 
 AFL_INSTANTIATE_STAGES(double)
 AFL_INSTANTIATE_FUSED(double)

@@ -49,18 +49,24 @@ template <typename T>
 void launch_advect_mc(const Dims &g, const T *u, const T *v, const T *w, const T *src,
                       const T *fwd, T *out, double dt, double dissipation, bool nonneg,
                       cudaStream_t st);
-// The shared-memory-staged forces stage (afl_stage_fused.cuh): curl,
-// confinement, buoyancy and the wall BC in one launch; the new velocity goes
-// to (uo, vo, wo), arrays distinct from (u, v, w).
+// The shared-memory-staged stage kernels (afl_stage_fused.cuh).
+// Density and temperature advected by (u, v, w) in one launch into out[]
+// (arrays distinct from the inputs), with the telemetry partials of the final
+// state in tel, 7 per CTA (fused_ctas of them).
+template <typename T>
+void launch_scalars_fused(const Dims &g, const T *u, const T *v, const T *w,
+                          const T *const src[2], T *const out[2], const double diss[2],
+                          double dt, double *tel, cudaStream_t st);
+// Curl, confinement, buoyancy and the wall BC in one launch; the new velocity
+// goes to (uo, vo, wo), arrays distinct from (u, v, w).
 template <typename T>
 void launch_forces_fused(const Dims &g, const T *u, const T *v, const T *w, const T *rho,
                          const T *temp, T *uo, T *vo, T *wo, double dt, double eps, double beta,
                          double alpha, cudaStream_t st);
-// True when a stage touching bytes_per_cell bytes per cell streams from HBM:
-// its arrays exceed twice the L2 cache of the current device.  Such grids run
-// the staged / vectorised stage kernels; smaller ones, which L2 serves, the
-// one-thread-per-cell kernels.
-bool streams_through_hbm(const Dims &g, size_t bytes_per_cell);
+int fused_ctas(const Dims &g);
+// Sums telemetry partials (7 per CTA) into the 8 doubles of compute_telemetry.
+void launch_telemetry_finalize(const double *partials, int nparts, double time_sec,
+                               double *out8, cudaStream_t st);
 template <typename T>
 void launch_wall_bc(const Dims &g, T *u, T *v, T *w, cudaStream_t st);
 template <typename T>

@@ -117,6 +117,7 @@ struct afl_solver {
   // Poisson vectors: FP64 -> r, d0, d1, q (double); MIXED -> r, e, d0, d1, q (float)
   void *cg[5] = {};
   double *partials = nullptr;     // kReduceBlocks * kReduceMaxVals
+  double *tel_partials = nullptr; // 7 per CTA of the fused density/temperature advection
   double *scal = nullptr;         // [0..1] divergence {rms,||b||}, [2..9] telemetry, [10] max
   double *tel = nullptr;          // run telemetry, 8 doubles per step
   afl::SolveReport *reports = nullptr;  // run reports, one per step
@@ -290,34 +291,41 @@ afl_status stage_wall_bc(afl_solver *s) {
   return launch_check();
 }
 
-// apply_buoyancy_and_vorticity_confinement (src/fluid.rs:256-330).  Grids
-// whose stage arrays exceed twice the L2 cache: one fused, shared-memory
-// staged launch writes the new velocity into three spare buffers, which then
-// become u, v, w (the curl never reaches memory).  Smaller grids, whose
-// arrays L2 holds: the curl kernel and the confinement kernel, one thread per
-// cell (at these sizes the extra curl traffic stays in L2 and the simple
-// kernels' occupancy wins).
+// apply_buoyancy_and_vorticity_confinement (src/fluid.rs:256-330): one
+// shared-memory-staged launch writes the new velocity into three spare
+// buffers, which then become u, v, w (the curl never reaches memory).
 template <typename T>
 afl_status stage_buoyancy_vorticity(afl_solver *s, double dt) {
-  if (afl::streams_through_hbm(s->g, 8 * sizeof(T))) {
-    StageTimer timer(s, AFL_STAGE_FORCES, 1);
-    afl::launch_forces_fused<T>(s->g, s->F<T>(0), s->F<T>(1), s->F<T>(2), s->F<T>(3),
-                                s->F<T>(4), static_cast<T *>(s->curl[0]),
-                                static_cast<T *>(s->curl[1]), static_cast<T *>(s->curl[2]), dt,
-                                s->params.vorticity_eps, s->params.buoyancy_beta,
-                                s->params.gravity_alpha, s->stream);
-    for (int f = 0; f < 3; ++f) std::swap(s->fld[f], s->curl[f]);
-    return launch_check();
+  StageTimer timer(s, AFL_STAGE_FORCES, 1);
+  afl::launch_forces_fused<T>(s->g, s->F<T>(0), s->F<T>(1), s->F<T>(2), s->F<T>(3), s->F<T>(4),
+                              static_cast<T *>(s->curl[0]), static_cast<T *>(s->curl[1]),
+                              static_cast<T *>(s->curl[2]), dt, s->params.vorticity_eps,
+                              s->params.buoyancy_beta, s->params.gravity_alpha, s->stream);
+  for (int f = 0; f < 3; ++f) std::swap(s->fld[f], s->curl[f]);
+  return launch_check();
+}
+
+// The end of step() (src/fluid.rs:607-610): density (dissipation 0.996) and
+// temperature (0.985) advected in one shared-memory-staged launch that reads
+// the velocity once and sums the telemetry of the final state; the finalize
+// kernel writes its 8 doubles.
+template <typename T>
+afl_status stage_advect_scalars_telemetry(afl_solver *s, double dt, double time_sec,
+                                          double *out8) {
+  const T *src[2] = {s->F<T>(3), s->F<T>(4)};
+  T *out[2] = {static_cast<T *>(s->tmp_out), static_cast<T *>(s->tmp_fwd)};
+  const double diss[2] = {0.996, 0.985};
+  {
+    StageTimer timer(s, AFL_STAGE_ADVECT, 1);
+    afl::launch_scalars_fused<T>(s->g, s->F<T>(0), s->F<T>(1), s->F<T>(2), src, out, diss, dt,
+                                 s->tel_partials, s->stream);
   }
-  T *c[4] = {static_cast<T *>(s->curl[0]), static_cast<T *>(s->curl[1]),
-             static_cast<T *>(s->curl[2]), static_cast<T *>(s->curl[3])};
-  StageTimer timer(s, AFL_STAGE_FORCES, 2);
-  afl::launch_curl<T>(s->g, s->F<T>(0), s->F<T>(1), s->F<T>(2), c[0], c[1], c[2], c[3],
-                      s->stream);
-  afl::launch_confine_buoy<T>(s->g, s->F<T>(0), s->F<T>(1), s->F<T>(2), s->F<T>(3),
-                              s->F<T>(4), c[0], c[1], c[2], c[3], dt,
-                              s->params.vorticity_eps, s->params.buoyancy_beta,
-                              s->params.gravity_alpha, s->stream);
+  std::swap(s->fld[3], s->tmp_out);
+  std::swap(s->fld[4], s->tmp_fwd);
+  AFL_TRY(launch_check());
+  StageTimer timer(s, AFL_STAGE_TELEMETRY, 1);
+  afl::launch_telemetry_finalize(s->tel_partials, afl::fused_ctas(s->g), time_sec, out8,
+                                 s->stream);
   return launch_check();
 }
 
@@ -474,9 +482,7 @@ afl_status stage_step(afl_solver *s, double dt, double time_sec, double *tel8,
   // The confinement kernel ends with the wall BC, so project's leading
   // enforce_wall_velocity_bc (src/fluid.rs:497) is a no-op here and skipped.
   AFL_TRY(stage_project<T>(s, false, rep));
-  AFL_TRY(stage_advect<T>(s, 3, dt, 0.996));
-  AFL_TRY(stage_advect<T>(s, 4, dt, 0.985));
-  return stage_telemetry<T>(s, time_sec, tel8);
+  return stage_advect_scalars_telemetry<T>(s, dt, time_sec, tel8);
 }
 
 template <typename Fn>
@@ -672,6 +678,8 @@ afl_status afl_create(size_t nx, size_t ny, size_t nz, const afl_params *params,
   if (st == AFL_OK)
     st = alloc_as(s, &s->partials, sizeof(double) * afl::kReduceBlocks * afl::kReduceMaxVals);
   if (st == AFL_OK) st = alloc_as(s, &s->scal, sizeof(double) * 16);
+  if (st == AFL_OK)
+    st = alloc_as(s, &s->tel_partials, sizeof(double) * 7 * afl::fused_ctas(s->g));
   if (st == AFL_OK) st = alloc_as(s, &s->sticky, sizeof(int) * 4);
   // persistent-kernel state: the CTA bound is the largest co-resident grid
   int maxb = std::max(std::max(afl::persistent_blocks_cg_f64(), afl::persistent_blocks_sor_f64()),

@@ -269,9 +269,8 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// The same stage with four cells per thread, for grids with nx % 128 == 0
-// whose arrays stream from HBM (smaller grids, which L2 serves, run
-// k_divergence): a warp covers 128 consecutive cells of a row and lane l takes cells l, l+32,
+// The same stage with four cells per thread (grids with nx % 128 == 0): a
+// warp covers 128 consecutive cells of a row and lane l takes cells l, l+32,
 // l+64 and l+96, so every load and store is coalesced and each thread has
 // four cells' loads in flight; the per-cell arithmetic is k_divergence's.  A
 // fixed grid of kReduceBlocks CTAs walks the rows, so the sums stay
@@ -364,8 +363,7 @@ __global__ void __launch_bounds__(kTx *kTy)
   });
 }
 
-// The same stage with four cells per thread, for grids with nx % 128 == 0
-// whose arrays stream from HBM (smaller grids run k_project): a warp covers
+// The same stage with four cells per thread (nx % 128 == 0): a warp covers
 // 128 consecutive cells of a row, lane l takes cells l, l+32, l+64 and
 // l+96, so every load and store is coalesced; cell_project's arithmetic.
 template <typename T>
@@ -591,7 +589,7 @@ template <typename T>
 void launch_divergence(const Dims &g, const T *u, const T *v, const T *w, double *b,
                        double *partials, double *out2, cudaStream_t st) {
   const double inv_h = 1.0 / g.h;
-  if (g.nx % 128 == 0 && streams_through_hbm(g, 3 * sizeof(T) + sizeof(double)))
+  if (g.nx % 128 == 0)
     k_divergence_x4<T><<<kReduceBlocks, kBlock, 0, st>>>(g, u, v, w, b, partials, inv_h, g.h);
   else
     k_divergence<T><<<kReduceBlocks, kBlock, 0, st>>>(g, u, v, w, b, partials, inv_h, g.h);
@@ -601,7 +599,7 @@ void launch_divergence(const Dims &g, const T *u, const T *v, const T *w, double
 
 template <typename T>
 void launch_project(const Dims &g, T *u, T *v, T *w, const double *p, cudaStream_t st) {
-  if (g.nx % 128 == 0 && streams_through_hbm(g, 6 * sizeof(T) + sizeof(double)))
+  if (g.nx % 128 == 0)
     k_project_x4<T><<<(g.n / 128 + kWarps - 1) / kWarps, kBlock, 0, st>>>(g, u, v, w, p,
                                                                           1.0 / g.h);
   else

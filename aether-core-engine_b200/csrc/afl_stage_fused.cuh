@@ -1,9 +1,6 @@
-// afl_stage_fused.cuh -- the shared-memory-staged form of the forces stage,
-// templated on the field type T (double: FP64 form; float: mixed form).
-// Included by afl_kernels_f64.cu (built with -fmad=false) and
-// afl_kernels_f32.cu.  The solver runs it on grids whose stage arrays exceed
-// twice the L2 cache, where the stage streams from HBM; smaller grids keep the
-// one-thread-per-cell kernels of afl_stage.cuh, which L2 serves faster.
+// afl_stage_fused.cuh -- the shared-memory-staged stage kernels, templated
+// on the field type T (double: FP64 form; float: mixed form).  Included by
+// afl_kernels_f64.cu (built with -fmad=false) and afl_kernels_f32.cu.
 //
 // Launch shape: one CTA of 256 threads owns a 32 x 8 tile of the x-y plane
 // (one thread per cell) and marches up a chunk of z planes.  Every plane it
@@ -14,12 +11,23 @@
 // rows reach 16 bytes past the tile on each side in x and two cells in y;
 // cells outside the grid read as 0.
 //
+// k_maccormack_fused: advect_maccormack_in_place (src/fluid.rs:170-234) in
+// one pass.  The forward semi-Lagrangian field `fwd` (:183) is computed on the
+// tile plus a one-cell halo into a ring of three shared planes; the backward
+// sample `bwd` (:184) reads that ring, and the clamp's 8-cell min/max
+// (:196-209) comes from the same staged corners as the cell's own `fwd`.  A
+// footprint that leaves the staged region (a backtrace longer than about one
+// cell) is evaluated from global memory with the same arithmetic.  The solver
+// uses it for the end of a step: density and temperature advected in one
+// launch that reads the velocity once, with the telemetry sums of the final
+// state (compute_telemetry, :613-672) accumulated in the same pass.
+//
 // k_forces_fused: apply_buoyancy_and_vorticity_confinement
 // (src/fluid.rs:256-330).  The curl and |w| of the tile plus a one-cell halo
 // exist only in shared memory and registers; the new velocities go to a
 // second set of arrays, because neighbouring CTAs still read the old ones.
-// Each cell's arithmetic is the expression of cell_curl and
-// cell_confine_buoy (afl_stage.cuh), so the FP64 results are the same bits.
+// Each cell's arithmetic is the expression of the per-cell kernels of
+// afl_stage.cuh, so the FP64 results are the same bits as theirs.
 #pragma once
 
 #include "afl_stage.cuh"
@@ -104,6 +112,47 @@ struct StageDesc {
   }
 };
 
+// Clamp bounds of sample_trilinear (src/fluid.rs:95-97) per axis, n - 1.500001,
+// computed once per CTA with the expression footprint3 uses.
+template <typename T>
+struct FpBounds {
+  T hx, hy, hz;
+  __device__ __forceinline__ explicit FpBounds(const Dims &g)
+      : hx(T(g.nx) - T(1.500001)), hy(T(g.ny) - T(1.500001)), hz(T(g.nz) - T(1.500001)) {}
+};
+
+// footprint3_at with the bounds precomputed: the same operations, so the same
+// corner and weights bit for bit.
+__device__ __forceinline__ void fp_axis(int i, double hi, double d, int &i0, double &t) {
+  const double xc = rs_clamp(double(i) - d, 0.5, hi);
+  i0 = static_cast<int>(floor(xc));
+  t = xc - double(i0);
+}
+__device__ __forceinline__ void fp_axis(int i, float hi, float d, int &i0, float &t) {
+  const float p = float(i) - d;
+  if (p < 0.5f) {
+    i0 = 0;
+    t = 0.5f;
+  } else if (p > hi) {
+    const float f = floorf(hi);
+    i0 = static_cast<int>(f);
+    t = hi - f;
+  } else {
+    const float f = floorf(-d);
+    i0 = i + static_cast<int>(f);
+    t = -d - f;
+  }
+}
+template <typename T>
+__device__ __forceinline__ Footprint3<T> fp_at(const FpBounds<T> &b, int i, int j, int k, T dx,
+                                               T dy, T dz) {
+  Footprint3<T> f;
+  fp_axis(i, b.hx, dx, f.i, f.tx);
+  fp_axis(j, b.hy, dy, f.j, f.ty);
+  fp_axis(k, b.hz, dz, f.k, f.tz);
+  return f;
+}
+
 // Cell t of the one-cell ring around the tile at (i0, j0).
 __device__ __forceinline__ void halo_cell(int t, int i0, int j0, int &i, int &j) {
   if (t < kFw) {
@@ -118,6 +167,310 @@ __device__ __forceinline__ void halo_cell(int t, int i0, int j0, int &i, int &j)
   } else {
     i = i0 + kFx;
     j = j0 + (t - 2 * kFw - kFy);
+  }
+}
+
+// ---- MacCormack advection ----------------------------------------------------
+template <typename T>
+struct McArgs {
+  Dims g;
+  const T *u, *v, *w;  // velocity (not written by the launch)
+  const T *src[2];     // advected fields
+  T *out[2];           // their new values (distinct arrays)
+  T scale_f, scale_b;  // dt/h and -dt/h
+  T diss[2];           // dissipation per field
+  int nonneg;          // density/temperature: max(0, .)
+  int vel_src;         // the advected field is velocity component vel_src (NF = 1)
+  int kz;              // z planes per CTA
+  double *tel;         // telemetry partials, 7 per CTA (TEL only)
+  double dv, inv_2h;   // telemetry: cell volume h^3 and 1/(2h)
+};
+
+template <typename T, int NF, bool SRC_IS_VEL>
+struct McLayout {
+  static constexpr int RW = Staged<T>::RW;
+  static constexpr int VYH = SRC_IS_VEL ? 2 : 1;       // y halo of the velocity rows
+  static constexpr int VROWS = kFy + 2 * VYH;
+  static constexpr int SROWS = kFy + 4;                // advected fields: y halo 2
+  static constexpr int VPL = 3 * VROWS * RW;           // one staged velocity plane
+  static constexpr int SPL = SRC_IS_VEL ? 0 : NF * SROWS * RW;
+  static constexpr int FPL = NF * kFh * kFw;           // one fwd plane
+  static constexpr int elems(int S) { return S * (VPL + SPL) + 3 * FPL; }
+};
+
+// One launch advects NF fields of the same velocity.  SRC_IS_VEL: the field
+// is a velocity component, read from the staged velocity (kept for
+// single-field use; the solver advects velocity with the fwd + mc pair of
+// afl_stage.cuh, which measured faster).  TEL (NF = 2, field 0 = density):
+// the telemetry sums over this CTA's cells go to a.tel[7 * cta] as
+// k_telemetry's partials.
+// Ring slots are tracked as plane offsets that advance by one slot per
+// iteration (no division); the plane pointers of an iteration are set once.
+template <typename T, int NF, bool SRC_IS_VEL, bool TEL, int S, bool VEC>
+__global__ void __launch_bounds__(kFThreads, NF == 1 ? 3 : 2)
+    k_maccormack_fused(const __grid_constant__ McArgs<T> a) {
+  static_assert(S >= 5, "the ring holds planes k-2 .. k+2 plus at least one ahead");
+  using L = McLayout<T, NF, SRC_IS_VEL>;
+  constexpr int RW = L::RW, XH = Staged<T>::XH, VYH = L::VYH, VROWS = L::VROWS;
+  constexpr int SROWS = L::SROWS, VPL = L::VPL, SPL = L::SPL, FPL = L::FPL;
+  constexpr int PL = VPL + SPL;  // one ring slot: the velocity, then the fields
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *ring = reinterpret_cast<T *>(smem_raw);
+  T *fring = ring + S * PL;
+  const Dims &g = a.g;
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.x * kFx, j0 = blockIdx.y * kFy;
+  const int k0 = blockIdx.z * a.kz;
+  const int k1 = min(k0 + a.kz, g.nz);
+  const int mi = i0 + (tid & (kFx - 1)), mj = j0 + tid / kFx;
+  const bool mine = mi < g.nx && mj < g.ny;
+  const FpBounds<T> fb_bounds(g);
+  const T wxl = T(1.5), wxh = T(g.nx) - T(2.5), wyh = T(g.ny) - T(2.5), wzh = T(g.nz) - T(2.5);
+  // field f of a slot starts SROWS*RW apart (velocity component vel_src when
+  // the field is a velocity component); rows start at y = j0 - 2
+  const int foff = SRC_IS_VEL ? a.vel_src * VROWS * RW : VPL;
+  constexpr int FSTRIDE = SROWS * RW;
+
+  const StageDesc<T, VEC> dvel(g, i0, j0, VYH);
+  const StageDesc<T, VEC> dsrc(g, i0, j0, 2);
+  auto stage = [&](T *slotp, int p) {
+    dvel.copy(slotp, a.u, g, p);
+    dvel.copy(slotp + VROWS * RW, a.v, g, p);
+    dvel.copy(slotp + 2 * VROWS * RW, a.w, g, p);
+    if constexpr (!SRC_IS_VEL) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) dsrc.copy(slotp + VPL + f * FSTRIDE, a.src[f], g, p);
+    }
+    cp_async_commit();
+  };
+  auto next_slot = [&](T *sp) { return sp + PL == ring + S * PL ? ring : sp + PL; };
+
+  // fwd = SL(src, dt) at cell (ci, cj) of plane p (advect_semi_lagrangian,
+  // src/fluid.rs:153-167) into fo of the fwd plane F.  vp: the staged plane
+  // p; vm, vq: planes p-1 and p+1 (for the field corners).  For the thread's
+  // own cell (own), also the min/max of the same 8 corners (stencil_minmax,
+  // :131-150), the bounds of its clamp.
+  auto fwd_cell = [&](int ci, int cj, int p, const T *vm, const T *vp, const T *vq, T *F,
+                      bool own, T (&lo)[NF], T (&hi)[NF]) {
+    T res[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) res[f] = T(0);
+    if (interior(g, ci, cj, p)) {
+      const int vo = (cj - j0 + VYH) * RW + (ci - i0 + XH);
+      const T uc = vp[vo], vc = vp[VROWS * RW + vo], wc = vp[2 * VROWS * RW + vo];
+      const Footprint3<T> fp =
+          fp_at(fb_bounds, ci, cj, p, a.scale_f * uc, a.scale_f * vc, a.scale_f * wc);
+      const bool staged = fp.i >= i0 - XH && fp.i + 1 < i0 + kFx + XH && fp.j >= j0 - 2 &&
+                          fp.j + 1 < j0 + kFy + 2 && fp.k >= p - 1 && fp.k <= p;
+      const int o = (fp.j - j0 + 2) * RW + (fp.i - i0 + XH) + foff;
+      const T *z0 = (fp.k == p - 1 ? vm : vp) + o;
+      const T *z1 = (fp.k == p - 1 ? vp : vq) + o;
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        T c[8];
+        if (staged) {
+          const T *s0 = z0 + f * FSTRIDE, *s1 = z1 + f * FSTRIDE;
+          c[0] = s0[0]; c[1] = s0[1]; c[2] = s0[RW]; c[3] = s0[RW + 1];
+          c[4] = s1[0]; c[5] = s1[1]; c[6] = s1[RW]; c[7] = s1[RW + 1];
+        } else {
+          const T *sg = a.src[f] + fp.base(g);
+          c[0] = __ldg(sg); c[1] = __ldg(sg + 1); c[2] = __ldg(sg + g.nx);
+          c[3] = __ldg(sg + g.nx + 1); c[4] = __ldg(sg + g.nxy); c[5] = __ldg(sg + g.nxy + 1);
+          c[6] = __ldg(sg + g.nxy + g.nx); c[7] = __ldg(sg + g.nxy + g.nx + 1);
+        }
+        res[f] = lerp8(c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], fp.tx, fp.ty, fp.tz);
+        if (own) {
+          T l = T(INFINITY), h = T(-INFINITY);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {  // minmax8's corner order
+            l = fmin(l, c[q]);
+            h = fmax(h, c[q]);
+          }
+          lo[f] = l;
+          hi[f] = h;
+        }
+      }
+    }
+    const int fo = (cj - j0 + 1) * kFw + (ci - i0 + 1);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) F[f * kFh * kFw + fo] = res[f];
+  };
+
+  // This thread's ring cell (threads below kFHalo), found once.
+  int hi_i = 0, hi_j = 0;
+  if (tid < kFHalo) halo_cell(tid, i0, j0, hi_i, hi_j);
+  // fwd of plane p on the tile and its one-cell ring (planes outside the grid
+  // are never sampled: every footprint lies inside it).
+  auto fwd_plane = [&](int p, const T *vm, const T *vp, const T *vq, T *F, T (&lo)[NF],
+                       T (&hi)[NF]) {
+    if (p < 0 || p >= g.nz) return;
+    if (mine) fwd_cell(mi, mj, p, vm, vp, vq, F, true, lo, hi);
+    if (tid < kFHalo) {
+      T dl[NF], dh[NF];
+      fwd_cell(hi_i, hi_j, p, vm, vp, vq, F, false, dl, dh);
+    }
+  };
+
+  // fwd at one cell from global memory: the fallback of a long backtrace.
+  auto fwd_global = [&](int f, int qi, int qj, int qk) -> T {
+    if (!interior(g, qi, qj, qk)) return T(0);
+    const int q = (qk * g.ny + qj) * g.nx + qi;
+    const T uq = __ldg(a.u + q), vq = __ldg(a.v + q), wq = __ldg(a.w + q);
+    return trilinear(a.src[f], g,
+                     footprint_at(g, qi, qj, qk, a.scale_f * uq, a.scale_f * vq, a.scale_f * wq));
+  };
+
+  T lo_cur[NF], hi_cur[NF], lo_nxt[NF], hi_nxt[NF];
+#pragma unroll
+  for (int f = 0; f < NF; ++f) lo_cur[f] = hi_cur[f] = lo_nxt[f] = hi_nxt[f] = T(0);
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  double peak = 0.0;
+
+  // slot of plane k0-2 is ring[0]; plane k0-2+t sits in slot t mod S
+  {
+    T *sp = ring;
+    for (int p = k0 - 2; p <= k0 + S - 3; ++p) {
+      stage(sp, p);
+      sp += PL;
+    }
+  }
+  T *sm2 = ring;                 // plane k-2 (k = k0)
+  T *sm1 = ring + PL;            // k-1
+  T *s0 = ring + 2 * PL;         // k
+  T *s1 = ring + 3 * PL;         // k+1
+  T *s2 = ring + 4 * PL;         // k+2
+  T *F0 = fring, *F1 = fring + FPL, *F2 = fring + 2 * FPL;  // fwd of planes k-1, k, k+1
+  cp_async_wait<S - 4>();  // planes k0-2 .. k0+1 have landed
+  __syncthreads();
+  fwd_plane(k0 - 1, sm2, sm1, s0, F0, lo_nxt, hi_nxt);  // ring plane only
+  fwd_plane(k0, sm1, s0, s1, F1, lo_cur, hi_cur);
+
+  for (int k = k0; k < k1; ++k) {
+    cp_async_wait<S - 5>();  // plane k+2 has landed
+    __syncthreads();         // ... for every thread; iteration k-1 is done with its planes
+    fwd_plane(k + 1, s0, s1, s2, F2, lo_nxt, hi_nxt);
+    __syncthreads();         // fwd of plane k+1 is visible
+    {
+      // plane k+S-2 goes into the slot of plane k-2, last read in iteration k-1
+      T *sp = sm2;
+      stage(sp, k + S - 2);
+    }
+    if (mine) {
+      T res[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) res[f] = T(0);
+      const int vo = (mj - j0 + VYH) * RW + (mi - i0 + XH);
+      const bool inner = interior(g, mi, mj, k);
+      if (inner) {
+        const T uc = s0[vo], vc = s0[VROWS * RW + vo], wc = s0[2 * VROWS * RW + vo];
+        const T bx = T(mi) - a.scale_f * uc;
+        const T by = T(mj) - a.scale_f * vc;
+        const T bz = T(k) - a.scale_f * wc;
+        const bool near_wall = bx < wxl || bx > wxh || by < wxl || by > wyh || bz < wxl ||
+                               bz > wzh;
+        const int fo = (mj - j0 + 1) * kFw + (mi - i0 + 1);
+        if (near_wall) {
+#pragma unroll
+          for (int f = 0; f < NF; ++f) res[f] = F1[f * kFh * kFw + fo] * a.diss[f];
+        } else {
+          const Footprint3<T> fb =
+              fp_at(fb_bounds, mi, mj, k, a.scale_b * uc, a.scale_b * vc, a.scale_b * wc);
+          const bool staged = fb.i >= i0 - 1 && fb.i + 1 <= i0 + kFx && fb.j >= j0 - 1 &&
+                              fb.j + 1 <= j0 + kFy && fb.k >= k - 1 && fb.k <= k;
+          const int o = (fb.j - j0 + 1) * kFw + (fb.i - i0 + 1);
+          const T *z0 = (fb.k == k - 1 ? F0 : F1) + o;
+          const T *z1 = (fb.k == k - 1 ? F1 : F2) + o;
+          const int so = (mj - j0 + 2) * RW + (mi - i0 + XH) + foff;
+#pragma unroll
+          for (int f = 0; f < NF; ++f) {
+            T bwd;
+            if (staged) {
+              const T *f0 = z0 + f * kFh * kFw, *f1 = z1 + f * kFh * kFw;
+              bwd = lerp8(f0[0], f0[1], f0[kFw], f0[kFw + 1], f1[0], f1[1], f1[kFw],
+                          f1[kFw + 1], fb.tx, fb.ty, fb.tz);
+            } else {
+              bwd = lerp8(fwd_global(f, fb.i, fb.j, fb.k), fwd_global(f, fb.i + 1, fb.j, fb.k),
+                          fwd_global(f, fb.i, fb.j + 1, fb.k),
+                          fwd_global(f, fb.i + 1, fb.j + 1, fb.k),
+                          fwd_global(f, fb.i, fb.j, fb.k + 1),
+                          fwd_global(f, fb.i + 1, fb.j, fb.k + 1),
+                          fwd_global(f, fb.i, fb.j + 1, fb.k + 1),
+                          fwd_global(f, fb.i + 1, fb.j + 1, fb.k + 1), fb.tx, fb.ty, fb.tz);
+            }
+            const T fc = F1[f * kFh * kFw + fo];
+            const T mc = fc + T(0.5) * (s0[so + f * FSTRIDE] - bwd);
+            res[f] = rs_clamp(mc, lo_cur[f], hi_cur[f]) * a.diss[f];
+          }
+        }
+      }
+      const int c = (k * g.ny + mj) * g.nx + mi;
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        if (a.nonneg) res[f] = fmax(res[f], T(0));
+        a.out[f][c] = res[f];
+      }
+      if constexpr (TEL) {
+        if (inner) {  // compute_telemetry (src/fluid.rs:613-672) at this cell
+          const T *U = s0, *Vv = s0 + VROWS * RW, *W = s0 + 2 * VROWS * RW;
+          const double uc = U[vo], vc = Vv[vo], wc = W[vo];
+          const double u2 = uc * uc + vc * vc + wc * wc;
+          acc[0] += 0.5 * u2 * a.dv;
+          const double dw_dy = (double(W[vo + RW]) - double(W[vo - RW])) * a.inv_2h;
+          const double dv_dz =
+              (double(s1[VROWS * RW + vo]) - double(sm1[VROWS * RW + vo])) * a.inv_2h;
+          const double du_dz = (double(s1[vo]) - double(sm1[vo])) * a.inv_2h;
+          const double dw_dx = (double(W[vo + 1]) - double(W[vo - 1])) * a.inv_2h;
+          const double dv_dx = (double(Vv[vo + 1]) - double(Vv[vo - 1])) * a.inv_2h;
+          const double du_dy = (double(U[vo + RW]) - double(U[vo - RW])) * a.inv_2h;
+          const double ox = dw_dy - dv_dz;
+          const double oy = du_dz - dw_dx;
+          const double oz = dv_dx - du_dy;
+          const double w2 = ox * ox + oy * oy + oz * oz;
+          acc[1] += 0.5 * w2 * a.dv;
+          peak = fmax(peak, sqrt(w2));
+          const double r = double(res[0]);
+          if (r > 1e-8) {
+            acc[2] += r * a.dv;
+            const double nxn = 2.0 * (double(mi) / double(g.nx - 1)) - 1.0;
+            const double nyn = 2.0 * (double(mj) / double(g.ny - 1)) - 1.0;
+            const double nzn = 2.0 * (double(k) / double(g.nz - 1)) - 1.0;
+            const double wgt = r * a.dv;
+            acc[3] += nxn * wgt;
+            acc[4] += nyn * wgt;
+            acc[5] += nzn * wgt;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      lo_cur[f] = lo_nxt[f];
+      hi_cur[f] = hi_nxt[f];
+    }
+    // advance the ring by one plane
+    T *old = sm2;
+    sm2 = sm1;
+    sm1 = s0;
+    s0 = s1;
+    s1 = s2;
+    s2 = next_slot(s2);
+    (void)old;
+    T *ft = F0;
+    F0 = F1;
+    F1 = F2;
+    F2 = ft;
+  }
+  cp_async_wait<0>();  // no copy outlives the CTA
+  if constexpr (TEL) {
+    __shared__ double scratch[kWarps * 6];
+    block_sum<6>(acc, scratch);
+    const double pk = block_max(peak, scratch);
+    if (tid == 0) {
+      const int cta = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) a.tel[cta * 7 + q] = acc[q];
+      a.tel[cta * 7 + 6] = pk;
+    }
   }
 }
 
@@ -271,7 +624,8 @@ __global__ void __launch_bounds__(kFThreads, 3)
 }
 
 // ---- launchers ------------------------------------------------------------------
-constexpr int kRingForces = 6;  // six planes: two ahead of the stencil's reach
+// Ring depths: six planes, two ahead of the stencils' reach.
+constexpr int kRingScalar = 6, kRingForces = 6;
 
 // z planes per CTA: about four waves of two resident CTAs per SM over the
 // grid, and at least 8 planes per CTA (the ring is primed with two planes
@@ -311,6 +665,16 @@ inline void fused_prepare(K kernel, size_t smem, unsigned long long &done_mask) 
 }
 
 template <typename T, bool VEC>
+void launch_scalars_variant(McArgs<T> a, cudaStream_t st) {
+  auto kern = k_maccormack_fused<T, 2, false, true, kRingScalar, VEC>;
+  const size_t smem = sizeof(T) * McLayout<T, 2, false>::elems(kRingScalar);
+  static unsigned long long prepared = 0;
+  fused_prepare(kern, smem, prepared);
+  a.kz = fused_kz(a.g);
+  kern<<<fused_grid(a.g, a.kz), kFThreads, smem, st>>>(a);
+}
+
+template <typename T, bool VEC>
 void launch_forces_variant(ForcesArgs<T> a, cudaStream_t st) {
   auto kern = k_forces_fused<T, kRingForces, VEC>;
   const size_t smem = sizeof(T) * ForcesLayout<T>::elems(kRingForces);
@@ -343,7 +707,46 @@ void launch_forces_fused(const Dims &g, const T *u, const T *v, const T *w, cons
   else launch_forces_variant<T, false>(a, st);
 }
 
+// CTAs of the fused density/temperature advection on this grid: the number
+// of telemetry partials it writes.
+inline int fused_ctas_of(const Dims &g) {
+  const dim3 gr = fused_grid(g, fused_kz(g));
+  return static_cast<int>(gr.x * gr.y * gr.z);
+}
+
+// advect_maccormack_in_place of density (dissipation diss[0]) and temperature
+// (diss[1]) by (u, v, w) in one launch, into out[0], out[1] (arrays distinct
+// from the inputs), max(0, .) applied; the telemetry partials of the final
+// state go to tel, 7 per CTA (fused_ctas of them).
+template <typename T>
+void launch_scalars_fused(const Dims &g, const T *u, const T *v, const T *w,
+                          const T *const src[2], T *const out[2], const double diss[2],
+                          double dt, double *tel, cudaStream_t st) {
+  McArgs<T> a{};
+  a.g = g;
+  a.u = u;
+  a.v = v;
+  a.w = w;
+  for (int f = 0; f < 2; ++f) {
+    a.src[f] = src[f];
+    a.out[f] = out[f];
+    a.diss[f] = T(diss[f]);
+  }
+  a.scale_f = T(dt / g.h);
+  a.scale_b = T((-dt) / g.h);
+  a.nonneg = 1;
+  a.vel_src = -1;
+  a.tel = tel;
+  a.dv = g.h * g.h * g.h;
+  a.inv_2h = 0.5 / g.h;
+  if (g.nx % Staged<T>::V == 0) launch_scalars_variant<T, true>(a, st);
+  else launch_scalars_variant<T, false>(a, st);
+}
+
 #define AFL_INSTANTIATE_FUSED(T)                                                           \
+  template void launch_scalars_fused<T>(const Dims &, const T *, const T *, const T *,      \
+                                        const T *const *, T *const *, const double *,       \
+                                        double, double *, cudaStream_t);                    \
   template void launch_forces_fused<T>(const Dims &, const T *, const T *, const T *,       \
                                        const T *, const T *, T *, T *, T *, double, double, \
                                        double, double, cudaStream_t);

@@ -95,9 +95,9 @@ def test_advection_tiles(af, oracle, shape, steps_per_cell, precision):
     same(g, o, ["u", "v", "w", "density", "temperature"], precision, tol=2e-6)
 
 
-# Grids whose stage arrays exceed twice the L2 cache, where the solver runs
-# the shared-memory-staged forces kernel (16-byte rows, and odd nx for the
-# element-wise copies) and the x4 divergence/projection kernels.
+# Grids far larger than L2 for the shared-memory-staged forces kernel (many z
+# chunks; 16-byte rows, and odd nx for the element-wise copies) and the x4
+# divergence/projection kernels (nx a multiple of 128).
 STREAM_FORCES = [((176, 160, 160), 0), ((177, 160, 160), 0), ((224, 200, 200), 1)]
 
 
