@@ -157,6 +157,8 @@ SIGNATURES = [
     ("afl_ensemble_instance_ctas", _st, [_vp, ctypes.POINTER(ctypes.c_int32), _i]),
     ("afl_ensemble_set_tile_depth", _st, [_vp, ctypes.c_int32]),
     ("afl_ensemble_tile_depth", _st, [_vp, ctypes.POINTER(ctypes.c_int32)]),
+    ("afl_ensemble_set_persistent", _st, [_vp, ctypes.c_int32]),
+    ("afl_ensemble_persistent", _st, [_vp, ctypes.POINTER(ctypes.c_int32)]),
     ("afl_rng_f64", _st, [ctypes.c_uint64, ctypes.c_uint64, _sz, _dp]),
     ("afl_adjoint_create", _st, [_sz, _sz, _sz, ctypes.POINTER(AflParams), _i,
                                  ctypes.POINTER(_vp)]),

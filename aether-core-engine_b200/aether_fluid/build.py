@@ -24,8 +24,8 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
           "--expt-relaxed-constexpr", "-extended-lambda"]
 # Units whose f64 arithmetic must not be contracted into FMAs.
 NO_FMA = {"afl_kernels_f64.cu", "afl_poisson_f64.cu", "afl_poisson_resident.cu",
-          "afl_poisson_stream.cu", "afl_ensemble_f64.cu", "afl_adjoint_kernels.cu",
-          "afl_medium.cu"}
+          "afl_poisson_stream.cu", "afl_ensemble_f64.cu", "afl_ensemble_persist.cu",
+          "afl_adjoint_kernels.cu", "afl_medium.cu"}
 SOURCES = [
     "afl_kernels_f64.cu",
     "afl_kernels_f32.cu",
@@ -37,6 +37,7 @@ SOURCES = [
     "afl_noalloc.cu",
     "afl_ensemble_f64.cu",
     "afl_ensemble_f32.cu",
+    "afl_ensemble_persist.cu",
     "afl_ensemble.cu",
     "afl_adjoint_kernels.cu",
     "afl_adjoint.cu",

@@ -146,10 +146,20 @@ class Ensemble:
         check(self._lib.afl_ensemble_instance_ctas(self._h, ctas, self.count))
         kz = ctypes.c_int32()
         check(self._lib.afl_ensemble_tile_depth(self._h, ctypes.byref(kz)))
+        pers = ctypes.c_int32()
+        check(self._lib.afl_ensemble_persistent(self._h, ctypes.byref(pers)))
         return {"instances": out[0], "graph": bool(out[1]), "solver_ctas": out[2],
                 "cta_budget": out[3], "vector_width": out[4], "autotune_choice": out[5],
-                "instance_ctas": list(ctas), "tile_depth": kz.value}
+                "instance_ctas": list(ctas), "tile_depth": kz.value,
+                "persistent": bool(pers.value)}
 
     def set_tile_depth(self, kz: int):
         """z planes per CTA tile of the batched stage kernels (1, 2 or 4)."""
         check(self._lib.afl_ensemble_set_tile_depth(self._h, kz))
+
+    def set_persistent(self, on: bool):
+        """Step form: False = the captured graph of per-stage batched launches
+        and the cooperative solve; True = one persistent cooperative launch per
+        step (instances meet only at their own barriers).  Re-splits the CTAs
+        for the form's co-resident budget and clears the autotune choice."""
+        check(self._lib.afl_ensemble_set_persistent(self._h, 1 if on else 0))

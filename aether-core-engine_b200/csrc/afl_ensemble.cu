@@ -5,9 +5,11 @@
 // -> instance descriptor -> the single-grid per-cell code), and the pressure
 // solves of all instances run in one cooperative launch whose CTAs are split
 // between the instances (afl_poisson_stream.cu, k_cg_stream_multi).  One step
-// is captured once into a CUDA graph and replayed.  The autotuner chooses the
-// CTA split of the batched solve by timing candidate splits on a snapshot of
-// the state, which it then restores.
+// is captured once into a CUDA graph and replayed.  Alternatively the whole
+// step runs as one persistent cooperative launch (afl_ensemble_persist.cu),
+// itself captured in the graph.  The autotuner chooses the CTA split of the
+// solve by timing candidate splits on a snapshot of the state, which it then
+// restores.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -119,6 +121,8 @@ struct afl_ensemble {
   // batched solve
   int vec = 1;
   int budget = 0;            // co-resident CTAs of the batched solve
+  int budget_step = 0;       // co-resident CTAs of the persistent step kernel
+  bool persistent = false;   // one persistent launch per step instead of the stage graph
   std::vector<int> ctas;     // per instance
   afl::MultiCgSystem *d_sys = nullptr;
   int *d_cta_inst = nullptr;
@@ -260,6 +264,9 @@ std::vector<int> split_ctas(const std::vector<double> &w, int budget) {
   return out;
 }
 
+// Co-resident CTAs of the launch that runs the solves in the current form.
+int active_budget(const afl_ensemble *e) { return e->persistent ? e->budget_step : e->budget; }
+
 afl_status build_systems(afl_ensemble *e, const std::vector<int> &ctas) {
   e->ctas = ctas;
   std::vector<afl::MultiCgSystem> sys(e->count);
@@ -318,6 +325,16 @@ afl_status enqueue_step(afl_ensemble *e) {
   afl::EnsLaunch<T> L{static_cast<afl::EnsInstance<T> *>(e->d_inst), e->d_blk_inst, e->blocks,
                       e->count};
   cudaStream_t st = e->stream;
+  if (e->persistent) {
+    ENS_CUDA(cudaMemsetAsync(e->d_bar, 0, sizeof(unsigned int) * (2 * e->count + 1), st));
+    afl::EnsStepArgs a{e->d_inst, e->d_sys,       e->d_cta_inst, e->d_tel_partials, e->d_step,
+                       e->d_tel_out, e->d_rep_cur, e->d_reports,  e->count,          e->capacity};
+    const int used = afl::launch_ens_step(a, e->f64, e->vec, e->total_ctas, st);
+    if (used <= 0) return cuda_fail(static_cast<cudaError_t>(-used), "persistent step launch");
+    afl::ens_step_advance(e->d_step, st);
+    ENS_CUDA(cudaGetLastError());
+    return AFL_OK;
+  }
   // step (src/fluid.rs:598-611) for every instance at once
   afl::ens_advect<T>(L, 0, 0.996, st);
   afl::ens_advect<T>(L, 1, 0.996, st);
@@ -526,11 +543,13 @@ afl_status afl_ensemble_create(const afl_instance *inst, int count, const afl_pa
   cudaMemset(e->d_step, 0, sizeof(int));
   // batched solve: every CTA co-resident; at least one CTA per instance
   e->budget = afl::persistent_blocks_multi(e->f64, e->vec);
+  e->budget_step = afl::persistent_blocks_ens_step(e->f64, e->vec);
   if (e->budget < count)
     return bail(fail(AFL_ERR_INVALID_ARGUMENT, "more instances than co-resident solver CTAs"));
   const int nv = e->f64 ? 2 : 3;
-  st = ens_alloc_as(e, &e->d_cta_inst, sizeof(int) * e->budget);
-  if (st == AFL_OK) st = ens_alloc_as(e, &e->d_cg_partials, sizeof(double) * 2 * nv * e->budget);
+  const int most = std::max(e->budget, e->budget_step);
+  st = ens_alloc_as(e, &e->d_cta_inst, sizeof(int) * most);
+  if (st == AFL_OK) st = ens_alloc_as(e, &e->d_cg_partials, sizeof(double) * 2 * nv * most);
   if (st != AFL_OK) return bail(st);
   std::vector<double> w(count);
   for (int m = 0; m < count; ++m) w[m] = static_cast<double>(e->dims[m].n);
@@ -665,7 +684,8 @@ afl_status afl_ensemble_autotune(afl_ensemble *e, int32_t *choice) {
   std::vector<double> cells(e->count), work(e->count);
   for (int m = 0; m < e->count; ++m) cells[m] = static_cast<double>(e->dims[m].n);
   std::vector<std::vector<int>> cands;
-  cands.push_back(split_ctas(cells, e->budget));
+  const int budget = active_budget(e);
+  cands.push_back(split_ctas(cells, budget));
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
@@ -686,8 +706,8 @@ afl_status afl_ensemble_autotune(afl_ensemble *e, int32_t *choice) {
   int best = 0, best_kz = kz0;
   afl_status st = AFL_OK;
   for (size_t c = 0; c < 3 && st == AFL_OK; ++c) {
-    if (c == 1) cands.push_back(split_ctas(work, e->budget));
-    if (c == 2) cands.push_back(split_ctas(cells, std::max(e->count, (3 * e->budget) / 4)));
+    if (c == 1) cands.push_back(split_ctas(work, budget));
+    if (c == 2) cands.push_back(split_ctas(cells, std::max(e->count, (3 * budget) / 4)));
     float ms = 0.0f;
     st = time_one(cands[c], 1, &ms);
     if (st != AFL_OK) break;
@@ -745,12 +765,33 @@ afl_status afl_ensemble_tile_depth(const afl_ensemble *e, int32_t *kz) {
   return AFL_OK;
 }
 
+afl_status afl_ensemble_set_persistent(afl_ensemble *e, int32_t on) {
+  if (!e) return fail(AFL_ERR_INVALID_ARGUMENT, "null ensemble");
+  if (on != 0 && on != 1) return fail(AFL_ERR_INVALID_ARGUMENT, "step form must be 0 or 1");
+  if (on && e->budget_step < e->count)
+    return fail(AFL_ERR_INVALID_ARGUMENT, "more instances than co-resident step-kernel CTAs");
+  ENS_CUDA(cudaStreamSynchronize(e->stream));
+  e->persistent = on != 0;
+  std::vector<double> w(e->count);
+  for (int m = 0; m < e->count; ++m) w[m] = static_cast<double>(e->dims[m].n);
+  ENS_TRY(build_systems(e, split_ctas(w, active_budget(e))));
+  e->tune_choice = -1;
+  build_graph(e);
+  return AFL_OK;
+}
+
+afl_status afl_ensemble_persistent(const afl_ensemble *e, int32_t *on) {
+  if (!e || !on) return fail(AFL_ERR_INVALID_ARGUMENT, "null argument");
+  *on = e->persistent ? 1 : 0;
+  return AFL_OK;
+}
+
 afl_status afl_ensemble_info(const afl_ensemble *e, int32_t out[6]) {
   if (!e || !out) return fail(AFL_ERR_INVALID_ARGUMENT, "null argument");
   out[0] = e->count;
   out[1] = e->graph_ok ? 1 : 0;
   out[2] = e->total_ctas;
-  out[3] = e->budget;
+  out[3] = active_budget(e);
   out[4] = e->vec;
   out[5] = e->tune_choice;
   return AFL_OK;

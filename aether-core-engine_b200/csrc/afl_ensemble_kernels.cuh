@@ -16,11 +16,11 @@
 
 namespace afl {
 
-// The cells of this CTA: a 32 x 8 tile of d.kz consecutive z planes of its
-// instance (the tile depth is the tuner's choice); body(i, j, k) per cell.
+// The cells of plane block `local` of an instance: a 32 x 8 tile of d.kz
+// consecutive z planes (the tile depth is the tuner's choice); body(i, j, k)
+// per cell, one cell per thread and plane.
 template <typename T, typename F>
-__device__ __forceinline__ void ens_cells(const EnsInstance<T> &d, F &&body) {
-  const int local = blockIdx.x - d.blk_begin;
+__device__ __forceinline__ void ens_cells_at(const EnsInstance<T> &d, int local, F &&body) {
   const int gx = (d.g.nx + kTx - 1) / kTx, gy = (d.g.ny + kTy - 1) / kTy;
   const int bx = local % gx, t = local / gx;
   const int by = t % gy;
@@ -33,39 +33,35 @@ __device__ __forceinline__ void ens_cells(const EnsInstance<T> &d, F &&body) {
   for (int k = k0; k < k1; ++k) body(i, j, k);
 }
 
+// The cells of this CTA's plane block (its index in the block table).
+template <typename T, typename F>
+__device__ __forceinline__ void ens_cells(const EnsInstance<T> &d, F &&body) {
+  ens_cells_at(d, static_cast<int>(blockIdx.x) - d.blk_begin, body);
+}
+
+// ---- per-block bodies ---------------------------------------------------------
+// Each body does one plane block (`local` within its instance); the batched
+// kernels below run one block per CTA, the persistent step kernel
+// (afl_ensemble_persist.cu) loops its CTAs over the blocks of their instance.
 template <typename T>
-__global__ void __launch_bounds__(kTx *kTy)
-    kb_advect_fwd(const EnsInstance<T> *inst, const int *blk_inst, int f) {
-  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
-  ens_cells(d, [&](int i, int j, int k) {
+__device__ __forceinline__ void blk_advect_fwd(const EnsInstance<T> &d, int local, int f) {
+  ens_cells_at(d, local, [&](int i, int j, int k) {
     cell_advect_fwd(d.g, d.fld[0], d.fld[1], d.fld[2], d.fld[f], d.tmp_fwd, d.scale_f, i, j, k);
   });
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kTx *kTy)
-    kb_advect_mc(const EnsInstance<T> *inst, const int *blk_inst, int f, double dissipation) {
-  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
-  ens_cells(d, [&](int i, int j, int k) {
+__device__ __forceinline__ void blk_advect_mc(const EnsInstance<T> &d, int local, int f,
+                                              double dissipation) {
+  ens_cells_at(d, local, [&](int i, int j, int k) {
     cell_advect_mc(d.g, d.fld[0], d.fld[1], d.fld[2], d.fld[f], d.tmp_fwd, d.tmp_out, d.scale_f,
                    d.scale_b, T(dissipation), f >= 3 ? 1 : 0, i, j, k);
   });
 }
 
-// The advected field becomes current; its old buffer becomes the next output.
 template <typename T>
-__global__ void kb_swap(EnsInstance<T> *inst, int count, int f) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= count) return;
-  T *t = inst[m].fld[f];
-  inst[m].fld[f] = inst[m].tmp_out;
-  inst[m].tmp_out = t;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kTx *kTy) kb_curl(const EnsInstance<T> *inst, const int *blk_inst) {
-  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
-  ens_cells(d, [&](int i, int j, int k) {
+__device__ __forceinline__ void blk_curl(const EnsInstance<T> &d, int local) {
+  ens_cells_at(d, local, [&](int i, int j, int k) {
     cell_curl(d.g, d.fld[0], d.fld[1], d.fld[2], d.curl[0], d.curl[1], d.curl[2], d.curl[3],
               d.inv_2h, i, j, k);
   });
@@ -76,10 +72,8 @@ __global__ void __launch_bounds__(kTx *kTy) kb_curl(const EnsInstance<T> *inst, 
 // temperature only at its own cell, after the assignment, as the separate
 // kernels do.
 template <typename T>
-__global__ void __launch_bounds__(kTx *kTy)
-    kb_source_confine_buoy(const EnsInstance<T> *inst, const int *blk_inst) {
-  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
-  ens_cells(d, [&](int i, int j, int k) {
+__device__ __forceinline__ void blk_source_confine_buoy(const EnsInstance<T> &d, int local) {
+  ens_cells_at(d, local, [&](int i, int j, int k) {
     const int c = (k * d.g.ny + j) * d.g.nx + i;
     T rho = d.fld[3][c], temp = d.fld[4][c];
     if (d.src_on && i >= d.src_lo[0] && i <= d.src_hi[0] && j >= d.src_lo[1] &&
@@ -102,10 +96,8 @@ __global__ void __launch_bounds__(kTx *kTy)
 
 // Right-hand side b = -h*(du+dv+dw) (src/fluid.rs:341-346), in f64.
 template <typename T>
-__global__ void __launch_bounds__(kTx *kTy)
-    kb_divergence(const EnsInstance<T> *inst, const int *blk_inst) {
-  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
-  ens_cells(d, [&](int i, int j, int k) {
+__device__ __forceinline__ void blk_divergence(const EnsInstance<T> &d, int local) {
+  ens_cells_at(d, local, [&](int i, int j, int k) {
     const int c = (k * d.g.ny + j) * d.g.nx + i;
     double bv = 0.0;
     if (interior(d.g, i, j, k)) {
@@ -120,24 +112,22 @@ __global__ void __launch_bounds__(kTx *kTy)
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kTx *kTy)
-    kb_project(const EnsInstance<T> *inst, const int *blk_inst) {
-  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
-  ens_cells(d, [&](int i, int j, int k) {
+__device__ __forceinline__ void blk_project(const EnsInstance<T> &d, int local) {
+  ens_cells_at(d, local, [&](int i, int j, int k) {
     cell_project(d.g, d.fld[0], d.fld[1], d.fld[2], d.p, d.inv_h, i, j, k);
   });
 }
 
-// compute_telemetry (src/fluid.rs:613-672): per-block partials of
-// (KE, enstrophy, mass, com x, com y, com z, peak |w|).
+// compute_telemetry (src/fluid.rs:613-672): the block's partials of
+// (KE, enstrophy, mass, com x, com y, com z, peak |w|) into
+// partials[(blk_begin + local) * 7 ...].  Block-wide: every thread of the CTA
+// calls it.
 template <typename T>
-__global__ void __launch_bounds__(kTx *kTy)
-    kb_telemetry(const EnsInstance<T> *inst, const int *blk_inst, double *partials) {
-  __shared__ double scratch[kWarps * 6];
-  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
+__device__ __forceinline__ void blk_telemetry(const EnsInstance<T> &d, int local,
+                                              double *partials, double *scratch) {
   double acc[6] = {0, 0, 0, 0, 0, 0};
   double peak = 0.0;
-  ens_cells(d, [&](int i, int j, int k) {
+  ens_cells_at(d, local, [&](int i, int j, int k) {
     if (!interior(d.g, i, j, k)) return;
     const Dims &g = d.g;
     const int c = (k * g.ny + j) * g.nx + i;
@@ -170,26 +160,23 @@ __global__ void __launch_bounds__(kTx *kTy)
   block_sum<6>(acc, scratch);
   const double pk = block_max(peak, scratch);
   if (threadIdx.x == 0) {
+    double *out = partials + static_cast<size_t>(d.blk_begin + local) * 7;
 #pragma unroll
-    for (int a = 0; a < 6; ++a) partials[blockIdx.x * 7 + a] = acc[a];
-    partials[blockIdx.x * 7 + 6] = pk;
+    for (int a = 0; a < 6; ++a) out[a] = acc[a];
+    out[6] = pk;
   }
 }
 
-// One CTA per instance: sums the instance's block partials in block order into
-// its telemetry frame of the current step, and files the step's solve report.
+// Sums instance m's block partials in block order into its telemetry frame of
+// step `step`, and files the step's solve report.  Block-wide, kBlock threads.
 template <typename T>
-__global__ void __launch_bounds__(kBlock)
-    kb_telemetry_finalize(const EnsInstance<T> *inst, const double *partials,
-                          const int *step_counter, double *tel_out,
-                          const SolveReport *rep_cur, SolveReport *reports, int count,
-                          int capacity) {
-  __shared__ double scratch[kWarps * 6];
-  const int m = blockIdx.x;
-  const EnsInstance<T> &d = inst[m];
+__device__ __forceinline__ void ens_finalize(const EnsInstance<T> &d, int m,
+                                             const double *partials, int step, double *tel_out,
+                                             const SolveReport *rep_cur, SolveReport *reports,
+                                             int count, int capacity, double *scratch) {
   double acc[6] = {0, 0, 0, 0, 0, 0};
   double peak = 0.0;
-  for (int b = threadIdx.x; b < d.blk_count; b += blockDim.x) {
+  for (int b = threadIdx.x; b < d.blk_count; b += kBlock) {
     const double *pp = partials + (d.blk_begin + b) * 7;
 #pragma unroll
     for (int a = 0; a < 6; ++a) acc[a] += pp[a];
@@ -197,7 +184,6 @@ __global__ void __launch_bounds__(kBlock)
   }
   block_sum<6>(acc, scratch);
   peak = block_max(peak, scratch);
-  const int step = *step_counter;
   if (threadIdx.x == 0 && step < capacity) {
     double *out = tel_out + (static_cast<size_t>(step) * count + m) * 8;
     const double mass = acc[2];
@@ -214,6 +200,79 @@ __global__ void __launch_bounds__(kBlock)
     for (int a = 0; a < 3; ++a) out[5 + a] = rs_clamp(com[a], -1.0, 1.0);
     reports[static_cast<size_t>(step) * count + m] = rep_cur[m];
   }
+}
+
+// ---- batched kernels: one plane block per CTA ---------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kTx *kTy)
+    kb_advect_fwd(const EnsInstance<T> *inst, const int *blk_inst, int f) {
+  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
+  blk_advect_fwd(d, static_cast<int>(blockIdx.x) - d.blk_begin, f);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTx *kTy)
+    kb_advect_mc(const EnsInstance<T> *inst, const int *blk_inst, int f, double dissipation) {
+  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
+  blk_advect_mc(d, static_cast<int>(blockIdx.x) - d.blk_begin, f, dissipation);
+}
+
+// The advected field becomes current; its old buffer becomes the next output.
+template <typename T>
+__global__ void kb_swap(EnsInstance<T> *inst, int count, int f) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= count) return;
+  T *t = inst[m].fld[f];
+  inst[m].fld[f] = inst[m].tmp_out;
+  inst[m].tmp_out = t;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTx *kTy) kb_curl(const EnsInstance<T> *inst, const int *blk_inst) {
+  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
+  blk_curl(d, static_cast<int>(blockIdx.x) - d.blk_begin);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTx *kTy)
+    kb_source_confine_buoy(const EnsInstance<T> *inst, const int *blk_inst) {
+  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
+  blk_source_confine_buoy(d, static_cast<int>(blockIdx.x) - d.blk_begin);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTx *kTy)
+    kb_divergence(const EnsInstance<T> *inst, const int *blk_inst) {
+  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
+  blk_divergence(d, static_cast<int>(blockIdx.x) - d.blk_begin);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTx *kTy)
+    kb_project(const EnsInstance<T> *inst, const int *blk_inst) {
+  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
+  blk_project(d, static_cast<int>(blockIdx.x) - d.blk_begin);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTx *kTy)
+    kb_telemetry(const EnsInstance<T> *inst, const int *blk_inst, double *partials) {
+  __shared__ double scratch[kWarps * 6];
+  const EnsInstance<T> &d = inst[blk_inst[blockIdx.x]];
+  blk_telemetry(d, static_cast<int>(blockIdx.x) - d.blk_begin, partials, scratch);
+}
+
+// One CTA per instance.
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    kb_telemetry_finalize(const EnsInstance<T> *inst, const double *partials,
+                          const int *step_counter, double *tel_out,
+                          const SolveReport *rep_cur, SolveReport *reports, int count,
+                          int capacity) {
+  __shared__ double scratch[kWarps * 6];
+  const int m = blockIdx.x;
+  ens_finalize(inst[m], m, partials, *step_counter, tel_out, rep_cur, reports, count, capacity,
+               scratch);
 }
 
 // ---- launchers -------------------------------------------------------------

@@ -274,6 +274,24 @@ void ens_telemetry(const EnsLaunch<T> &L, double *partials, const int *step_coun
                    int capacity, cudaStream_t st);
 void ens_step_advance(int *step_counter, cudaStream_t st);
 
+// One persistent cooperative launch for a whole ensemble step
+// (afl_ensemble_persist.cu): CTA b works on instance cta_inst[b] with the CTA
+// range, barrier and partials of sys[cta_inst[b]].
+struct EnsStepArgs {
+  void *inst;                 // EnsInstance<T>[count] (device)
+  const MultiCgSystem *sys;   // per instance: solve arguments, barrier, CTA range
+  const int *cta_inst;        // CTA -> instance
+  double *tel_partials;       // 7 per plane block
+  const int *step_counter;
+  double *tel_out;
+  const SolveReport *rep_cur;
+  SolveReport *reports;
+  int count, capacity;
+};
+// Co-resident CTAs of the step kernel for the precision and run width v.
+int persistent_blocks_ens_step(bool f64, int v);
+int launch_ens_step(const EnsStepArgs &a, bool f64, int v, int total_ctas, cudaStream_t st);
+
 // Occupancy-derived CTA count of each persistent kernel (co-residency bound).
 int persistent_blocks_cg_f64();
 int persistent_blocks_sor_f64();

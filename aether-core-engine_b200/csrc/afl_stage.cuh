@@ -12,6 +12,14 @@
 
 #include "afl_launch.h"
 
+// Pointer qualifier of the per-cell code.  A unit that runs several stages in
+// one launch, reading in a later stage what an earlier one wrote, defines it
+// empty before including this header, so that no load of such data can be
+// taken through the read-only (non-coherent) data path.
+#ifndef AFL_RESTRICT
+#define AFL_RESTRICT __restrict__
+#endif
+
 namespace afl {
 
 constexpr int kTx = 32, kTy = 8;
@@ -54,10 +62,10 @@ __device__ __forceinline__ void for_column_cells(const Dims &g, F &&body) {
 // ---- MacCormack advection (src/fluid.rs:153-234) ---------------------------
 // Pass 1: fwd = SL(src, dt) -- advect_semi_lagrangian (src/fluid.rs:153-167).
 template <typename T>
-__device__ __forceinline__ void cell_advect_fwd(const Dims &g, const T *__restrict__ u,
-                                                const T *__restrict__ v,
-                                                const T *__restrict__ w,
-                                                const T *__restrict__ src, T *__restrict__ fwd,
+__device__ __forceinline__ void cell_advect_fwd(const Dims &g, const T *AFL_RESTRICT u,
+                                                const T *AFL_RESTRICT v,
+                                                const T *AFL_RESTRICT w,
+                                                const T *AFL_RESTRICT src, T *AFL_RESTRICT fwd,
                                                 T scale, int i, int j, int k) {
   const int c = (k * g.ny + j) * g.nx + i;
   T out = T(0);
@@ -69,8 +77,8 @@ __device__ __forceinline__ void cell_advect_fwd(const Dims &g, const T *__restri
 
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
-    k_advect_fwd(Dims g, const T *__restrict__ u, const T *__restrict__ v,
-                 const T *__restrict__ w, const T *__restrict__ src, T *__restrict__ fwd,
+    k_advect_fwd(Dims g, const T *AFL_RESTRICT u, const T *AFL_RESTRICT v,
+                 const T *AFL_RESTRICT w, const T *AFL_RESTRICT src, T *AFL_RESTRICT fwd,
                  T scale) {
   for_column_cells(g, [&](int i, int j, int k) {
     cell_advect_fwd(g, u, v, w, src, fwd, scale, i, j, k);
@@ -82,11 +90,11 @@ __global__ void __launch_bounds__(kTx *kTy)
 // near-wall fallback, dissipation and max(0) for scalars (:186-229).  The
 // result goes to a separate buffer: src is read at data-dependent cells.
 template <typename T>
-__device__ __forceinline__ void cell_advect_mc(const Dims &g, const T *__restrict__ u,
-                                               const T *__restrict__ v,
-                                               const T *__restrict__ w,
-                                               const T *__restrict__ src,
-                                               const T *__restrict__ fwd, T *__restrict__ out,
+__device__ __forceinline__ void cell_advect_mc(const Dims &g, const T *AFL_RESTRICT u,
+                                               const T *AFL_RESTRICT v,
+                                               const T *AFL_RESTRICT w,
+                                               const T *AFL_RESTRICT src,
+                                               const T *AFL_RESTRICT fwd, T *AFL_RESTRICT out,
                                                T scale_f, T scale_b, T dissipation, int nonneg,
                                                int i, int j, int k) {
   const int c = (k * g.ny + j) * g.nx + i;
@@ -120,9 +128,9 @@ __device__ __forceinline__ void cell_advect_mc(const Dims &g, const T *__restric
 
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
-    k_advect_mc(Dims g, const T *__restrict__ u, const T *__restrict__ v,
-                const T *__restrict__ w, const T *__restrict__ src,
-                const T *__restrict__ fwd, T *__restrict__ out, T scale_f, T scale_b,
+    k_advect_mc(Dims g, const T *AFL_RESTRICT u, const T *AFL_RESTRICT v,
+                const T *AFL_RESTRICT w, const T *AFL_RESTRICT src,
+                const T *AFL_RESTRICT fwd, T *AFL_RESTRICT out, T scale_f, T scale_b,
                 T dissipation, int nonneg) {
   for_column_cells(g, [&](int i, int j, int k) {
     cell_advect_mc(g, u, v, w, src, fwd, out, scale_f, scale_b, dissipation, nonneg, i, j, k);
@@ -132,7 +140,7 @@ __global__ void __launch_bounds__(kTx *kTy)
 // ---- enforce_wall_velocity_bc (src/fluid.rs:236-253) -----------------------
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
-    k_wall_bc(Dims g, T *__restrict__ u, T *__restrict__ v, T *__restrict__ w) {
+    k_wall_bc(Dims g, T *AFL_RESTRICT u, T *AFL_RESTRICT v, T *AFL_RESTRICT w) {
   for_column_cells(g, [&](int i, int j, int k) {
     const int c = (k * g.ny + j) * g.nx + i;
     if (wall_u(g, i, j, k)) u[c] = T(0);
@@ -144,10 +152,10 @@ __global__ void __launch_bounds__(kTx *kTy)
 // ---- vorticity confinement + buoyancy (src/fluid.rs:256-330) ---------------
 // Pass 1: central-difference curl and |omega| on the interior (:260-281).
 template <typename T>
-__device__ __forceinline__ void cell_curl(const Dims &g, const T *__restrict__ u,
-                                          const T *__restrict__ v, const T *__restrict__ w,
-                                          T *__restrict__ cx, T *__restrict__ cy,
-                                          T *__restrict__ cz, T *__restrict__ cmag, T inv_2h,
+__device__ __forceinline__ void cell_curl(const Dims &g, const T *AFL_RESTRICT u,
+                                          const T *AFL_RESTRICT v, const T *AFL_RESTRICT w,
+                                          T *AFL_RESTRICT cx, T *AFL_RESTRICT cy,
+                                          T *AFL_RESTRICT cz, T *AFL_RESTRICT cmag, T inv_2h,
                                           int i, int j, int k) {
   const int c = (k * g.ny + j) * g.nx + i;
   if (!interior(g, i, j, k)) {
@@ -175,9 +183,9 @@ __device__ __forceinline__ void cell_curl(const Dims &g, const T *__restrict__ u
 
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
-    k_curl(Dims g, const T *__restrict__ u, const T *__restrict__ v,
-           const T *__restrict__ w, T *__restrict__ cx, T *__restrict__ cy,
-           T *__restrict__ cz, T *__restrict__ cmag, T inv_2h) {
+    k_curl(Dims g, const T *AFL_RESTRICT u, const T *AFL_RESTRICT v,
+           const T *AFL_RESTRICT w, T *AFL_RESTRICT cx, T *AFL_RESTRICT cy,
+           T *AFL_RESTRICT cz, T *AFL_RESTRICT cmag, T inv_2h) {
   for_column_cells(g, [&](int i, int j, int k) {
     cell_curl(g, u, v, w, cx, cy, cz, cmag, inv_2h, i, j, k);
   });
@@ -187,12 +195,12 @@ __global__ void __launch_bounds__(kTx *kTy)
 // (:318-327) and the wall BC (:329), fused; pointwise in u/v/w, so in place.
 // `rho_c`/`temp_c` are the density and temperature at the cell.
 template <typename T>
-__device__ __forceinline__ void cell_confine_buoy(const Dims &g, T *__restrict__ u,
-                                                  T *__restrict__ v, T *__restrict__ w,
-                                                  T rho_c, T temp_c, const T *__restrict__ cx,
-                                                  const T *__restrict__ cy,
-                                                  const T *__restrict__ cz,
-                                                  const T *__restrict__ cmag, T dt, T eps_h,
+__device__ __forceinline__ void cell_confine_buoy(const Dims &g, T *AFL_RESTRICT u,
+                                                  T *AFL_RESTRICT v, T *AFL_RESTRICT w,
+                                                  T rho_c, T temp_c, const T *AFL_RESTRICT cx,
+                                                  const T *AFL_RESTRICT cy,
+                                                  const T *AFL_RESTRICT cz,
+                                                  const T *AFL_RESTRICT cmag, T dt, T eps_h,
                                                   T inv_2h, T beta, T alpha, int i, int j,
                                                   int k) {
   const int c = (k * g.ny + j) * g.nx + i;
@@ -223,10 +231,10 @@ __device__ __forceinline__ void cell_confine_buoy(const Dims &g, T *__restrict__
 
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
-    k_confine_buoy(Dims g, T *__restrict__ u, T *__restrict__ v, T *__restrict__ w,
-                   const T *__restrict__ rho, const T *__restrict__ temp,
-                   const T *__restrict__ cx, const T *__restrict__ cy,
-                   const T *__restrict__ cz, const T *__restrict__ cmag, T dt, T eps_h,
+    k_confine_buoy(Dims g, T *AFL_RESTRICT u, T *AFL_RESTRICT v, T *AFL_RESTRICT w,
+                   const T *AFL_RESTRICT rho, const T *AFL_RESTRICT temp,
+                   const T *AFL_RESTRICT cx, const T *AFL_RESTRICT cy,
+                   const T *AFL_RESTRICT cz, const T *AFL_RESTRICT cmag, T dt, T eps_h,
                    T inv_2h, T beta, T alpha) {
   for_column_cells(g, [&](int i, int j, int k) {
     const int c = (k * g.ny + j) * g.nx + i;
@@ -241,9 +249,9 @@ __global__ void __launch_bounds__(kTx *kTy)
 // count; per-CTA partials of (sum div^2, sum b^2).
 template <typename T>
 __global__ void __launch_bounds__(kBlock)
-    k_divergence(Dims g, const T *__restrict__ u, const T *__restrict__ v,
-                 const T *__restrict__ w, double *__restrict__ b,
-                 double *__restrict__ partials, double inv_h, double h) {
+    k_divergence(Dims g, const T *AFL_RESTRICT u, const T *AFL_RESTRICT v,
+                 const T *AFL_RESTRICT w, double *AFL_RESTRICT b,
+                 double *AFL_RESTRICT partials, double inv_h, double h) {
   __shared__ double scratch[kWarps * 2];
   double acc[2] = {0.0, 0.0};
 #pragma unroll 2
@@ -277,9 +285,9 @@ __global__ void __launch_bounds__(kBlock)
 // reproducible.
 template <typename T>
 __global__ void __launch_bounds__(kBlock)
-    k_divergence_x4(Dims g, const T *__restrict__ u, const T *__restrict__ v,
-                    const T *__restrict__ w, double *__restrict__ b,
-                    double *__restrict__ partials, double inv_h, double h) {
+    k_divergence_x4(Dims g, const T *AFL_RESTRICT u, const T *AFL_RESTRICT v,
+                    const T *AFL_RESTRICT w, double *AFL_RESTRICT b,
+                    double *AFL_RESTRICT partials, double inv_h, double h) {
   __shared__ double scratch[kWarps * 2];
   double acc[2] = {0.0, 0.0};
   const int lane = threadIdx.x & 31;
@@ -330,17 +338,17 @@ __global__ void __launch_bounds__(kBlock)
 
 // Finishes k_divergence: out2 = {RMS divergence, ||b||_2}.
 __global__ void __launch_bounds__(kBlock)
-    k_divergence_finalize(const double *__restrict__ partials, int nparts,
-                          double interior_cells, double *__restrict__ out2);
+    k_divergence_finalize(const double *AFL_RESTRICT partials, int nparts,
+                          double interior_cells, double *AFL_RESTRICT out2);
 
 // ---- projection (src/fluid.rs:509-528) -------------------------------------
 // u -= (p[i]-p[i-1])/h where i > 1 (likewise v, w), then the wall BC.  The
 // gradient is formed in f64; in the mixed form the f32 velocity is updated in
 // f64 and rounded once.
 template <typename T>
-__device__ __forceinline__ void cell_project(const Dims &g, T *__restrict__ u,
-                                             T *__restrict__ v, T *__restrict__ w,
-                                             const double *__restrict__ p, double inv_h, int i,
+__device__ __forceinline__ void cell_project(const Dims &g, T *AFL_RESTRICT u,
+                                             T *AFL_RESTRICT v, T *AFL_RESTRICT w,
+                                             const double *AFL_RESTRICT p, double inv_h, int i,
                                              int j, int k) {
   const int c = (k * g.ny + j) * g.nx + i;
   if (interior(g, i, j, k)) {
@@ -356,8 +364,8 @@ __device__ __forceinline__ void cell_project(const Dims &g, T *__restrict__ u,
 
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
-    k_project(Dims g, T *__restrict__ u, T *__restrict__ v, T *__restrict__ w,
-              const double *__restrict__ p, double inv_h) {
+    k_project(Dims g, T *AFL_RESTRICT u, T *AFL_RESTRICT v, T *AFL_RESTRICT w,
+              const double *AFL_RESTRICT p, double inv_h) {
   for_column_cells(g, [&](int i, int j, int k) {
     cell_project(g, u, v, w, p, inv_h, i, j, k);
   });
@@ -368,8 +376,8 @@ __global__ void __launch_bounds__(kTx *kTy)
 // l+96, so every load and store is coalesced; cell_project's arithmetic.
 template <typename T>
 __global__ void __launch_bounds__(kBlock)
-    k_project_x4(Dims g, T *__restrict__ u, T *__restrict__ v, T *__restrict__ w,
-                 const double *__restrict__ p, double inv_h) {
+    k_project_x4(Dims g, T *AFL_RESTRICT u, T *AFL_RESTRICT v, T *AFL_RESTRICT w,
+                 const double *AFL_RESTRICT p, double inv_h) {
   const int lane = threadIdx.x & 31;
   const int sgi = (blockIdx.x * kBlock + threadIdx.x) / 32;
   if (sgi >= g.n / 128) return;
@@ -415,9 +423,9 @@ __global__ void __launch_bounds__(kBlock)
 // overlap.  pulse and the jet geometry are computed on the host.
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
-    k_inject_jet(Dims g, int i0, int j0, int k0, int ni, int nj, T *__restrict__ rho,
-                 T *__restrict__ temp, T *__restrict__ u, T *__restrict__ v,
-                 T *__restrict__ w, double jx, double jy, double jz, double vx, double vy,
+    k_inject_jet(Dims g, int i0, int j0, int k0, int ni, int nj, T *AFL_RESTRICT rho,
+                 T *AFL_RESTRICT temp, T *AFL_RESTRICT u, T *AFL_RESTRICT v,
+                 T *AFL_RESTRICT w, double jx, double jy, double jz, double vx, double vy,
                  double vz, double r2, double dt, double pulse) {
   const int ii = blockIdx.x * kTx + threadIdx.x;
   const int jj = blockIdx.y * kTy + threadIdx.y;
@@ -440,8 +448,8 @@ __global__ void __launch_bounds__(kTx *kTy)
 // Sphere source: density/temperature assignment inside the sphere.
 template <typename T>
 __global__ void __launch_bounds__(kTx *kTy)
-    k_inject_sphere(Dims g, int i0, int j0, int k0, int ni, int nj, T *__restrict__ rho,
-                    T *__restrict__ temp, const double *__restrict__ amp, double cx,
+    k_inject_sphere(Dims g, int i0, int j0, int k0, int ni, int nj, T *AFL_RESTRICT rho,
+                    T *AFL_RESTRICT temp, const double *AFL_RESTRICT amp, double cx,
                     double cy, double cz, double r2, double rho_val, double temp_val) {
   const int ii = blockIdx.x * kTx + threadIdx.x;
   const int jj = blockIdx.y * kTy + threadIdx.y;
@@ -461,9 +469,9 @@ __global__ void __launch_bounds__(kTx *kTy)
 // Per-CTA partials of (KE, enstrophy, mass, com x, com y, com z, peak |w|).
 template <typename T>
 __global__ void __launch_bounds__(kBlock)
-    k_telemetry(Dims g, const T *__restrict__ u, const T *__restrict__ v,
-                const T *__restrict__ w, const T *__restrict__ rho,
-                double *__restrict__ partials, double dv, double inv_2h) {
+    k_telemetry(Dims g, const T *AFL_RESTRICT u, const T *AFL_RESTRICT v,
+                const T *AFL_RESTRICT w, const T *AFL_RESTRICT rho,
+                double *AFL_RESTRICT partials, double dv, double inv_2h) {
   __shared__ double scratch[kWarps * 6];
   double acc[6] = {0, 0, 0, 0, 0, 0};
   double peak = 0.0;
@@ -515,12 +523,12 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 __global__ void __launch_bounds__(kBlock)
-    k_telemetry_finalize(const double *__restrict__ partials, int nparts, double time_sec,
-                         double *__restrict__ out8);
+    k_telemetry_finalize(const double *AFL_RESTRICT partials, int nparts, double time_sec,
+                         double *AFL_RESTRICT out8);
 
 template <typename T>
 __global__ void __launch_bounds__(kBlock)
-    k_max(int n, const T *__restrict__ x, double *__restrict__ partials) {
+    k_max(int n, const T *AFL_RESTRICT x, double *AFL_RESTRICT partials) {
   __shared__ double scratch[kWarps];
   double m = 0.0;  // max_density starts at 0 (src/fluid.rs:704)
   for (int c = blockIdx.x * kBlock + threadIdx.x; c < n; c += gridDim.x * kBlock)
@@ -530,13 +538,13 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 __global__ void __launch_bounds__(kBlock)
-    k_max_finalize(const double *__restrict__ partials, int nparts, double *__restrict__ out1);
+    k_max_finalize(const double *AFL_RESTRICT partials, int nparts, double *AFL_RESTRICT out1);
 
 // Batched sample_trilinear (src/fluid.rs:94-128) at caller-given points.
 template <typename T>
 __global__ void __launch_bounds__(kBlock)
-    k_sample(Dims g, const T *__restrict__ f, const double *__restrict__ xyz, int npts,
-             double *__restrict__ out) {
+    k_sample(Dims g, const T *AFL_RESTRICT f, const double *AFL_RESTRICT xyz, int npts,
+             double *AFL_RESTRICT out) {
   const int t = blockIdx.x * kBlock + threadIdx.x;
   if (t >= npts) return;
   const T x = T(xyz[3 * t]), y = T(xyz[3 * t + 1]), z = T(xyz[3 * t + 2]);

@@ -54,18 +54,23 @@ def test_ensemble_matches_single_solvers(af, precision, tol):
         assert all(abs(a - b) <= 1 for a, b in zip(its, its1)), (m, its, its1)
 
 
+@pytest.mark.parametrize("persistent", [False, True])
 @pytest.mark.parametrize("precision,tol", [(0, 1e-8), (1, 1e-4)])
-def test_ensemble_matches_oracle(af, oracle, precision, tol):
+def test_ensemble_matches_oracle(af, oracle, precision, tol, persistent):
     """Every instance of a batched ensemble of four grid sizes against its own
     run of the f64 CPU oracle (src/fluid.rs:598-611 with the sphere source):
     the fields after 5 steps within 1e-8 relative L2 (FP64; the batched CG
     sums in another order) or 1e-4 (mixed), and, in FP64, the per-step CG
-    iteration counts within 1."""
+    iteration counts within 1.  Both step forms: the graph of stage launches
+    and the single persistent launch."""
     from aether_fluid.ensemble import Ensemble
     O = oracle
     specs = specs_small()
     steps = 5
     ens = Ensemble(specs, precision=precision)
+    if persistent:
+        ens.set_persistent(True)
+        assert ens.info()["persistent"] and ens.info()["graph"]
     tel, infos = ens.run(steps)
     for m, spec in enumerate(specs):
         o = O.OracleSolver(spec.nx, spec.ny, spec.nz)
@@ -157,3 +162,55 @@ def test_tile_depth_does_not_change_the_evolution(af, kz):
     b.run(2)
     for m in range(len(specs)):
         assert np.array_equal(a.field(m, "density"), b.field(m, "density"))
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-10), (1, 1e-5)])
+def test_persistent_step_matches_stage_graph(af, precision, tol):
+    """One persistent launch per step against the graph of per-stage launches:
+    the same per-cell code and CG body, so the fields agree to the summation
+    order of the CG (its CTA split follows the step kernel's co-resident
+    budget) and, in f32, to FMA contraction (the step kernel's unit is built
+    without it).  Switching the form mid-run continues from the current state."""
+    from aether_fluid.ensemble import Ensemble
+    specs = specs_small()
+    a = Ensemble(specs, precision=precision)
+    tel_a, infos_a = a.run(5)
+    b = Ensemble(specs, precision=precision)
+    b.set_persistent(True)
+    info = b.info()
+    assert info["persistent"] and info["graph"], info
+    assert sum(info["instance_ctas"]) == info["solver_ctas"] <= info["cta_budget"]
+    tel_b, infos_b = b.run(2)
+    b.set_persistent(False)
+    assert not b.info()["persistent"]
+    tel_c, infos_c = b.run(1)
+    b.set_persistent(True)
+    tel_d, infos_d = b.run(2)
+    tel_bd = np.concatenate([tel_b, tel_c, tel_d])
+    infos_bd = infos_b + infos_c + infos_d
+    for m in range(len(specs)):
+        for f in FIELDS:
+            err = rel_l2(b.field(m, f), a.field(m, f))
+            assert err <= tol, (m, f, err)
+        its_a = [infos_a[n][m].iterations for n in range(5)]
+        its_b = [infos_bd[n][m].iterations for n in range(5)]
+        assert all(abs(x - y) <= 1 for x, y in zip(its_a, its_b)), (m, its_a, its_b)
+    # run() restarts the step count: each run's frames are numbered from 0
+    np.testing.assert_allclose(tel_bd[:, :, 1:5], tel_a[:, :, 1:5], rtol=max(tol, 1e-9))
+
+
+def test_persistent_autotune_restores_state(af):
+    from aether_fluid.ensemble import Ensemble
+    specs = specs_small()
+    a = Ensemble(specs, precision=1)
+    a.set_persistent(True)
+    choice = a.autotune()
+    info = a.info()
+    assert choice in (0, 1, 2) and info["autotune_choice"] == choice and info["persistent"]
+    tel_a, _ = a.run(3)
+    b = Ensemble(specs, precision=1)
+    b.set_persistent(True)
+    tel_b, _ = b.run(3)
+    for m in range(len(specs)):
+        for f in ("density", "u"):
+            assert rel_l2(a.field(m, f), b.field(m, f)) <= 1e-5
