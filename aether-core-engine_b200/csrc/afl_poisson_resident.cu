@@ -117,8 +117,8 @@ __device__ __forceinline__ void tag_publish(const TagSync &ts, unsigned int tag,
 }
 
 // The fixed-order total of sum number `tag` over all CTAs, in every thread.
-// Thread b waits for CTA b's words (relaxed loads; a fence after the wait
-// makes it an acquire of what CTA b released) and parks the value in shared
+// Thread b waits for CTA b's words (relaxed loads; an acquire load after the
+// wait makes it an acquire of what CTA b released) and parks the value in shared
 // `vals`; then warp 0 lane l adds CTAs l, l+32, ... in that order and a
 // butterfly combines the lanes, so every CTA computes the same bits.  Waits
 // are bounded like grid_sync's (abort flag and clock polled every 256 spins; a
@@ -157,9 +157,14 @@ __device__ __forceinline__ bool tag_gather(const TagSync &ts, const GridSync &gs
     for (int a = 0; a < NV; ++a)
       vals[b * NV + a] = __longlong_as_double(
           static_cast<long long>((w[2 * a + 1] << 32) | (w[2 * a] & 0xffffffffull)));
-    // acquire: plain loads after the sum (halo values of other CTAs) must see
-    // the writes released with it
-    __threadfence();
+    // acquire: loads after the sum (halo values of other CTAs) must see the
+    // writes released with it.  An acquire load of a word already seen with
+    // this tag synchronises with CTA b's release without the full fence,
+    // which would also wait for this thread's own outstanding stores.
+    {
+      unsigned long long t;
+      asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(t) : "l"(src) : "memory");
+    }
   }
   ok = __syncthreads_and(ok);
   if (threadIdx.x < 32) {
