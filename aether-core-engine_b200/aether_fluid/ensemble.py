@@ -1,7 +1,8 @@
 """Batched ensembles of independent smoke plumes (include/aether_fluid.h,
-afl_ensemble_*): every stage of a step is one launch over all instances, the
-pressure solves share one cooperative launch, and a step is a replayed CUDA
-graph."""
+afl_ensemble_*): by default a step is one persistent cooperative launch over
+all instances; the other form runs every stage as one launch over all
+instances with the pressure solves in one cooperative launch.  Either way a
+step is a replayed CUDA graph."""
 from __future__ import annotations
 
 import ctypes
@@ -158,8 +159,8 @@ class Ensemble:
         check(self._lib.afl_ensemble_set_tile_depth(self._h, kz))
 
     def set_persistent(self, on: bool):
-        """Step form: False = the captured graph of per-stage batched launches
-        and the cooperative solve; True = one persistent cooperative launch per
-        step (instances meet only at their own barriers).  Re-splits the CTAs
+        """Step form: True (the default) = one persistent cooperative launch
+        per step (instances meet only at their own barriers); False = the
+        captured graph of per-stage batched launches and the cooperative solve.  Re-splits the CTAs
         for the form's co-resident budget and clears the autotune choice."""
         check(self._lib.afl_ensemble_set_persistent(self._h, 1 if on else 0))

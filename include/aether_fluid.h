@@ -296,10 +296,11 @@ afl_status afl_ensemble_instance_ctas(const afl_ensemble *e, int32_t *out, int c
  * the solver's CTA split; these set and read it directly. */
 afl_status afl_ensemble_set_tile_depth(afl_ensemble *e, int32_t kz);
 afl_status afl_ensemble_tile_depth(const afl_ensemble *e, int32_t *kz);
-/* Step form: 0 = the captured graph of per-stage batched launches plus the
- * cooperative solve (the default); 1 = one persistent cooperative launch per
- * step, the CTAs of each instance meeting at the instance's own bounded
- * barrier between stages.  Setting it re-splits the CTAs for the form's
+/* Step form: 1 = one persistent cooperative launch per step, the CTAs of
+ * each instance meeting at the instance's own bounded barrier between stages
+ * (the default when the step kernel's co-resident CTAs outnumber the
+ * instances); 0 = the captured graph of per-stage batched launches plus the
+ * cooperative solve.  Setting it re-splits the CTAs for the form's
  * co-resident budget, clears the autotune choice and captures the step again. */
 afl_status afl_ensemble_set_persistent(afl_ensemble *e, int32_t on);
 afl_status afl_ensemble_persistent(const afl_ensemble *e, int32_t *on);

@@ -68,9 +68,8 @@ def test_ensemble_matches_oracle(af, oracle, precision, tol, persistent):
     specs = specs_small()
     steps = 5
     ens = Ensemble(specs, precision=precision)
-    if persistent:
-        ens.set_persistent(True)
-        assert ens.info()["persistent"] and ens.info()["graph"]
+    ens.set_persistent(persistent)
+    assert ens.info()["persistent"] == persistent and ens.info()["graph"]
     tel, infos = ens.run(steps)
     for m, spec in enumerate(specs):
         o = O.OracleSolver(spec.nx, spec.ny, spec.nz)
@@ -174,8 +173,10 @@ def test_persistent_step_matches_stage_graph(af, precision, tol):
     from aether_fluid.ensemble import Ensemble
     specs = specs_small()
     a = Ensemble(specs, precision=precision)
+    a.set_persistent(False)
     tel_a, infos_a = a.run(5)
     b = Ensemble(specs, precision=precision)
+    assert b.info()["persistent"]       # the default form
     b.set_persistent(True)
     info = b.info()
     assert info["persistent"] and info["graph"], info
