@@ -61,6 +61,14 @@ struct Footprint {
 
 // The same footprint with the corner as three indices (the fused stage
 // kernels test whether it lies inside their shared-memory tile).
+// floor(x) as a cell index.  A NaN position (a field that has blown up)
+// gives cell 0, as the reference's `as usize` does, instead of an index that
+// the float-to-int conversion leaves undefined.
+template <typename T>
+__device__ __forceinline__ int floor_index(T x) {
+  return x == x ? static_cast<int>(floor(x)) : 0;
+}
+
 template <typename T>
 struct Footprint3 {
   int i, j, k;  // corner (i0, j0, k0)
@@ -74,9 +82,9 @@ __device__ __forceinline__ Footprint3<T> footprint3(const Dims &g, T x, T y, T z
   const T yc = rs_clamp(y, T(0.5), T(g.ny) - T(1.500001));
   const T zc = rs_clamp(z, T(0.5), T(g.nz) - T(1.500001));
   Footprint3<T> f;
-  f.i = static_cast<int>(floor(xc));
-  f.j = static_cast<int>(floor(yc));
-  f.k = static_cast<int>(floor(zc));
+  f.i = floor_index(xc);
+  f.j = floor_index(yc);
+  f.k = floor_index(zc);
   f.tx = xc - T(f.i);
   f.ty = yc - T(f.j);
   f.tz = zc - T(f.k);
@@ -134,7 +142,10 @@ __device__ __forceinline__ Footprint3<T> footprint3_at(const Dims &g, int i, int
 __device__ __forceinline__ void axis_at(int i, int n, float d, int &i0, float &t) {
   const float p = float(i) - d;
   const float hi = float(n) - 1.500001f;
-  if (p < 0.5f) {
+  if (!(p == p)) {  // NaN displacement: cell 0, as floor_index
+    i0 = 0;
+    t = p;
+  } else if (p < 0.5f) {
     i0 = 0;
     t = 0.5f;
   } else if (p > hi) {

@@ -61,9 +61,9 @@ __device__ __forceinline__ void sample_dt(const MediumDev &m, V3 p, double &rho,
   const double gx = rs_clamp(ux * double(m.g.nx - 1), 0.5, double(m.g.nx) - 1.500001);
   const double gy = rs_clamp(uy * double(m.g.ny - 1), 0.5, double(m.g.ny) - 1.500001);
   const double gz = rs_clamp(uz * double(m.g.nz - 1), 0.5, double(m.g.nz) - 1.500001);
-  const int i0 = static_cast<int>(floor(gx));
-  const int j0 = static_cast<int>(floor(gy));
-  const int k0 = static_cast<int>(floor(gz));
+  const int i0 = afl::floor_index(gx);
+  const int j0 = afl::floor_index(gy);
+  const int k0 = afl::floor_index(gz);
   const double tx = gx - double(i0), ty = gy - double(j0), tz = gz - double(k0);
   const int b = (k0 * m.g.ny + j0) * m.g.nx + i0, sy = m.g.nx, sz = m.g.nxy;
   auto trilin = [&](const double *f) {

@@ -125,12 +125,15 @@ struct FpBounds {
 // corner and weights bit for bit.
 __device__ __forceinline__ void fp_axis(int i, double hi, double d, int &i0, double &t) {
   const double xc = rs_clamp(double(i) - d, 0.5, hi);
-  i0 = static_cast<int>(floor(xc));
+  i0 = floor_index(xc);
   t = xc - double(i0);
 }
 __device__ __forceinline__ void fp_axis(int i, float hi, float d, int &i0, float &t) {
   const float p = float(i) - d;
-  if (p < 0.5f) {
+  if (!(p == p)) {  // NaN displacement: cell 0, as floor_index
+    i0 = 0;
+    t = p;
+  } else if (p < 0.5f) {
     i0 = 0;
     t = 0.5f;
   } else if (p > hi) {

@@ -374,3 +374,51 @@ def test_resident_sor_matches_streaming(af, shape, precision):
         assert np.array_equal(out["resident"], out["streaming"])
     else:
         assert rel_l2(out["resident"], out["streaming"]) <= 1e-5
+
+
+@pytest.mark.parametrize("shape", [(40, 36, 30), (64, 24, 40)])
+@pytest.mark.parametrize("kind", [0, 3])
+def test_nan_velocity_cell_matches_oracle(af, oracle, shape, kind):
+    """A velocity field that has blown up (a NaN at an interior cell): the
+    backtrace of that cell has a NaN position, which the reference's
+    `floor() as usize` turns into cell 0.  FP64 advection gives the oracle's
+    fields, NaNs in the same places, and the handle stays usable."""
+    g, o = pair(af, oracle, shape, seed=7, vel_scale=1.0)
+    nx, ny, nz = shape
+    c = ((nz // 2) * ny + ny // 2) * nx + nx // 2
+    for s in (g, o):
+        if s is g:
+            u = g.get_field("u")
+            u[c] = np.nan
+            g.set_field("u", u)
+        else:
+            o.field("u")[c] = np.nan
+    dt = 1.5 * g.h
+    g.advect_maccormack_in_place(kind, dt, 0.985)
+    o.advect_maccormack_in_place(kind, dt, 0.985)
+    name = ("u", "v", "w", "density", "temperature")[kind]
+    for f in (name, "u", "v", "w"):
+        a, ref = g.get_field(f), o.field(f)
+        assert np.array_equal(a, ref, equal_nan=True), (f, np.isnan(a).sum(), np.isnan(ref).sum())
+    g.advect_maccormack_in_place(1, dt, 0.985)   # the handle still runs kernels
+
+
+@pytest.mark.parametrize("kind", [0, 3])
+def test_nan_velocity_cell_mixed_runs(af, kind):
+    """The same in the mixed form (its f32 backtrace takes the corner from the
+    displacement): the kernels run, and the NaN reaches only the cells whose
+    samples include it."""
+    shape = (40, 36, 30)
+    g = af.FluidSolver3D(*shape, precision=1)
+    st = seeded_state(shape, 7, 1.0)
+    for f, vals in st.items():
+        g.set_field(f, vals)
+    u = g.get_field("u")
+    c = (15 * 36 + 18) * 40 + 20
+    u[c] = np.nan
+    g.set_field("u", u)
+    g.advect_maccormack_in_place(kind, 1.5 * g.h, 0.985)
+    name = ("u", "v", "w", "density", "temperature")[kind]
+    out = g.get_field(name)
+    assert np.isnan(out).sum() < out.size // 100
+    g.advect_maccormack_in_place(1, 1.5 * g.h, 0.985)
