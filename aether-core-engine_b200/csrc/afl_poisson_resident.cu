@@ -591,14 +591,18 @@ __device__ __forceinline__ void cg_f64_body(const ResidentCgArgs &a, const GridS
       // p += alpha d, r -= alpha q, d = r + beta d (src/fluid.rs:472-485)
       double *const rw = odd ? rpub0 : rpub1;
       rr_next = 0.0;
+      // q of a chunk comes from L2; the next chunk's loads are issued after
+      // this chunk's TMEM stores, when its r and p registers are free, so their
+      // latency overlaps the next TMEM loads (holding them longer spills)
+      double qn[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        qn[q] = (q < CPT && cl.valid(g, q)) ? __ldcg(qw + cl.c0 + q * g.nxy) : 0.0;
 #pragma unroll 1
       for (int ch = 0; ch < NCH; ++ch) {
         double rv4[4], pv4[4], qv4[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int m = ch * 4 + q;
-          qv4[q] = (m < CPT && cl.valid(g, m)) ? __ldcg(qw + cl.c0 + m * g.nxy) : 0.0;
-        }
+        for (int q = 0; q < 4; ++q) qv4[q] = qn[q];
         tm_ld4(t_r + 8u * ch, rv4);
         tm_ld4(t_p + 8u * ch, pv4);
 #pragma unroll
@@ -616,6 +620,13 @@ __device__ __forceinline__ void cg_f64_body(const ResidentCgArgs &a, const GridS
         }
         tm_st4(t_r + 8u * ch, rv4);
         tm_st4(t_p + 8u * ch, pv4);
+        if (ch + 1 < NCH) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int m = (ch + 1) * 4 + q;
+            qn[q] = (m < CPT && cl.valid(g, m)) ? __ldcg(qw + cl.c0 + m * g.nxy) : 0.0;
+          }
+        }
       }
       const double *const rr_ring = odd ? rpub1 : rpub0;
       halo.fill_rolled(g, D, [&](int c, double dprev) {
