@@ -167,9 +167,8 @@ struct ResidentCgArgs {
   double *p;            // f64 pressure
   const double *b;      // f64 right-hand side
   void *rpub;           // mixed: published tile-edge residual (f32, n cells).
-                        // FP64: the first of four consecutive arrays of n
-                        // doubles: tile-edge r by iteration parity (0, 1), then
-                        // q = A d by parity (0, 1)
+                        // FP64: 4n doubles: the (r, q = A d) pair of every
+                        // cell, by iteration parity (0, 1)
   void *dpub0, *dpub1;  // mixed: published tile-edge direction, by iteration parity
   int max_iters;        // FP64: CG iterations; mixed: inner iterations, all passes
   int max_inner;        // mixed: inner iterations per refinement pass

@@ -452,8 +452,9 @@ __device__ __forceinline__ void tm_st4(unsigned taddr, const double (&v)[4]) {
 // tolerance extension, one grid-wide sum per iteration.
 //  * d lives in shared memory (tile + halo ring); the residual r and the
 //    pressure p live in tensor memory (TMEM); q = A d goes to global memory
-//    (L2) by iteration parity, where the neighbours also read its tile-edge
-//    values.  With r and p off the register file the kernel does not spill.
+//    (L2) with r as a (r, q) pair by iteration parity, where the neighbours
+//    also read the tile-edge pairs.  With r and p off the register file the
+//    kernel does not spill.
 //  * One sum carries d.q, r.q, q.q and the r.r of the current residual.
 //    alpha = delta/(d.q) takes the true delta = r.r; the next r.r, which the
 //    reference sums after r -= alpha q, is the same number expanded,
@@ -463,8 +464,8 @@ __device__ __forceinline__ void tm_st4(unsigned taddr, const double (&v)[4]) {
 //    the next iteration's sum: the test runs there, before any further update,
 //    so the iterations done and the stopping iteration are the reference's.
 //  * The halo ring of d' = (r - alpha q) + beta d is rebuilt from the
-//    neighbours' published r and q (written before the sum) with the owner's
-//    expression, bit for bit.  r edges and q are kept by iteration parity.
+//    neighbours' published (r, q) pairs (written before the sum) with the
+//    owner's expression, bit for bit.  The pairs are kept by iteration parity.
 //  * The stencil marches up each thread's column with the z neighbours in
 //    registers and no selects (d is exactly 0 off the interior).
 // The arguments are __grid_constant__: they stay in the constant bank.
@@ -479,10 +480,11 @@ __device__ __forceinline__ void cg_f64_body(const ResidentCgArgs &a, const GridS
   const C cl(g, a.tiles_x);
   const Halo<TY> halo(g, a.tiles_x);
   double *p = a.p;
-  double *const rpub0 = static_cast<double *>(a.rpub);
-  double *const rpub1 = rpub0 + g.n;
-  double *const q0 = rpub0 + 2 * static_cast<size_t>(g.n);
-  double *const q1 = rpub0 + 3 * static_cast<size_t>(g.n);
+  // (r, q) of every cell by iteration parity: the stencil pass publishes the
+  // pair once (one 16-byte store), the update reloads its own q from it and
+  // the ring rebuild reads both halves with one load
+  double2 *const pr0 = static_cast<double2 *>(a.rpub);
+  double2 *const pr1 = pr0 + g.n;
   int phase = 0;
   {
     // r = b - A p (src/fluid.rs:455-458) and p into TMEM, d = r.  The chunk
@@ -502,7 +504,7 @@ __device__ __forceinline__ void cg_f64_body(const ResidentCgArgs &a, const GridS
           const double rv = bc - ap;
           rv4[q] = rv;
           pv4[q] = __ldcg(p + c);
-          if (cl.edge) rpub0[c] = rv;
+          if (cl.edge) pr0[c].x = rv;
           acc[0] += rv * rv;
           acc[1] += bc * bc;
         }
@@ -530,12 +532,12 @@ __device__ __forceinline__ void cg_f64_body(const ResidentCgArgs &a, const GridS
     converged = isfinite(delta) ? 1 : 0;
   } else {
     // the first direction on the halo ring: the neighbours' r
-    halo.fill_rolled(g, D, [&](int c, double) { return __ldcg(rpub0 + c); });
+    halo.fill_rolled(g, D, [&](int c, double) { return __ldcg(&pr0[c].x); });
     __syncthreads();
     double rr_next = 0.0;
     for (;;) {
       const bool odd = (it & 1) != 0;
-      double *const qw = odd ? q1 : q0;
+      double2 *const pw = odd ? pr1 : pr0;
       // q = A d (src/fluid.rs:465) marching up the column (the z neighbours in
       // registers, the neighbour sum in the reference's order x-, x+, y-, y+,
       // z-, z+, no selects); d.q, r.q, q.q; this residual's r.r
@@ -565,7 +567,7 @@ __device__ __forceinline__ void cg_f64_body(const ResidentCgArgs &a, const GridS
             acc[0] += mid * qk;
             acc[1] += rc[q] * qk;
             acc[2] += qk * qk;
-            if (cl.valid(g, m)) qw[cl.c0 + m * g.nxy] = qk;
+            if (cl.valid(g, m)) pw[cl.c0 + m * g.nxy] = make_double2(rc[q], qk);
             below = mid;
             mid = above;
             s += C::SXY;
@@ -589,7 +591,6 @@ __device__ __forceinline__ void cg_f64_body(const ResidentCgArgs &a, const GridS
       const double dnext = delta - 2.0 * alpha * sum[1] + alpha * alpha * sum[2];
       const double beta = dnext / delta;
       // p += alpha d, r -= alpha q, d = r + beta d (src/fluid.rs:472-485)
-      double *const rw = odd ? rpub0 : rpub1;
       rr_next = 0.0;
       // q of a chunk comes from L2; the next chunk's loads are issued after
       // this chunk's TMEM stores, when its r and p registers are free, so their
@@ -597,7 +598,7 @@ __device__ __forceinline__ void cg_f64_body(const ResidentCgArgs &a, const GridS
       double qn[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        qn[q] = (q < CPT && cl.valid(g, q)) ? __ldcg(qw + cl.c0 + q * g.nxy) : 0.0;
+        qn[q] = (q < CPT && cl.valid(g, q)) ? __ldcg(&pw[cl.c0 + q * g.nxy].y) : 0.0;
 #pragma unroll 1
       for (int ch = 0; ch < NCH; ++ch) {
         double rv4[4], pv4[4], qv4[4];
@@ -616,7 +617,6 @@ __device__ __forceinline__ void cg_f64_body(const ResidentCgArgs &a, const GridS
           rv4[q] = rv;
           D[s] = rv + beta * dv;
           rr_next += rv * rv;
-          if (cl.edge && cl.valid(g, m)) rw[cl.c0 + m * g.nxy] = rv;
         }
         tm_st4(t_r + 8u * ch, rv4);
         tm_st4(t_p + 8u * ch, pv4);
@@ -624,13 +624,14 @@ __device__ __forceinline__ void cg_f64_body(const ResidentCgArgs &a, const GridS
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             const int m = (ch + 1) * 4 + q;
-            qn[q] = (m < CPT && cl.valid(g, m)) ? __ldcg(qw + cl.c0 + m * g.nxy) : 0.0;
+            qn[q] = (m < CPT && cl.valid(g, m)) ? __ldcg(&pw[cl.c0 + m * g.nxy].y) : 0.0;
           }
         }
       }
-      const double *const rr_ring = odd ? rpub1 : rpub0;
+
       halo.fill_rolled(g, D, [&](int c, double dprev) {
-        const double rv = __ldcg(rr_ring + c) - alpha * __ldcg(qw + c);
+        const double2 v = __ldcg(pw + c);
+        const double rv = v.x - alpha * v.y;
         return rv + beta * dprev;
       });
       __syncthreads();
