@@ -592,19 +592,19 @@ __device__ __forceinline__ void cg_f64_body(const ResidentCgArgs &a, const GridS
       const double beta = dnext / delta;
       // p += alpha d, r -= alpha q, d = r + beta d (src/fluid.rs:472-485)
       rr_next = 0.0;
-      // q of a chunk comes from L2; the next chunk's loads are issued after
-      // this chunk's TMEM stores, when its r and p registers are free, so their
-      // latency overlaps the next TMEM loads (holding them longer spills)
-      double qn[4];
+      // r and q of a chunk come from this thread's published pairs in L2 (r
+      // as in TMEM, bit for bit); the next chunk's loads are issued after this
+      // chunk's TMEM stores, when its registers are free, so their latency
+      // overlaps the next TMEM load (holding them longer spills)
+      double2 qn[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        qn[q] = (q < CPT && cl.valid(g, q)) ? __ldcg(&pw[cl.c0 + q * g.nxy].y) : 0.0;
+        qn[q] = (q < CPT && cl.valid(g, q)) ? __ldcg(&pw[cl.c0 + q * g.nxy]) : make_double2(0.0, 0.0);
 #pragma unroll 1
       for (int ch = 0; ch < NCH; ++ch) {
         double rv4[4], pv4[4], qv4[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) qv4[q] = qn[q];
-        tm_ld4(t_r + 8u * ch, rv4);
+        for (int q = 0; q < 4; ++q) { rv4[q] = qn[q].x; qv4[q] = qn[q].y; }
         tm_ld4(t_p + 8u * ch, pv4);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -624,7 +624,7 @@ __device__ __forceinline__ void cg_f64_body(const ResidentCgArgs &a, const GridS
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             const int m = (ch + 1) * 4 + q;
-            qn[q] = (m < CPT && cl.valid(g, m)) ? __ldcg(&pw[cl.c0 + m * g.nxy].y) : 0.0;
+            qn[q] = (m < CPT && cl.valid(g, m)) ? __ldcg(&pw[cl.c0 + m * g.nxy]) : make_double2(0.0, 0.0);
           }
         }
       }
