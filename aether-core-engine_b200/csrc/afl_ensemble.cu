@@ -7,7 +7,7 @@
 // between the instances (afl_poisson_stream.cu, k_cg_stream_multi).  One step
 // is captured once into a CUDA graph and replayed.  By default the whole step
 // instead runs as one persistent cooperative launch (afl_ensemble_persist.cu),
-// itself captured in the graph; it measured 2-3 % faster on the 48-plume
+// itself captured in the graph; it measured 0-5 % faster on the 48-plume
 // ensemble.  The autotuner chooses the CTA split of the
 // solve by timing candidate splits on a snapshot of the state, which it then
 // restores.
