@@ -463,8 +463,12 @@ __device__ __forceinline__ bool cg_stream_mixed_body(const MixedCgArgs &a, const
         spmv_run<float, V, DirF32>(g, ru, r, dold, first, bf, dn, qv);
         stv<float, V>(dnew + ru.c, dn);
         if (!SINGLE) stv<float, V>(q + ru.c, qv);
+        {  // the run's products summed in f32, the runs in f64 (256^3: 706 -> 722)
+          float part = 0.0f;
 #pragma unroll
-        for (int x = 0; x < V; ++x) acc[0] += double(dn.v[x]) * double(qv.v[x]);
+          for (int x = 0; x < V; ++x) part = __fmaf_rn(dn.v[x], qv.v[x], part);
+          acc[0] += double(part);
+        }
       }
       cta_publish<1>(pr.buf(phase), vblock, acc, scratch);
       if (!grid_sync(gs)) return false;
@@ -490,12 +494,14 @@ __device__ __forceinline__ bool cg_stream_mixed_body(const MixedCgArgs &a, const
         if (!SINGLE) qv = ldv<float, V>(q + c);
         else lap_run<float, V>(g, ru, dnew, dv, qv);
         Vec<float, V> rv = ldv<float, V>(r + c);
+        float part = 0.0f;
 #pragma unroll
         for (int x = 0; x < V; ++x) {
           ev.v[x] = __fmaf_rn(af, dv.v[x], ev.v[x]);
           rv.v[x] = __fmaf_rn(-af, qv.v[x], rv.v[x]);
-          acc2[0] += double(rv.v[x]) * double(rv.v[x]);
+          part = __fmaf_rn(rv.v[x], rv.v[x], part);
         }
+        acc2[0] += double(part);
         stv<float, V>(e + c, ev);
         stv<float, V>(r + c, rv);
       }
